@@ -1,0 +1,609 @@
+// api.cu -- the C ABI of include/sbfs.h.
+//
+// Host flow of one sbfs_solve_batch call (the native counterpart of
+// GPGPU/GPU/SlimGPUQueue.cs:32-208, which allocates, flattens and copies per
+// call, launches one kernel per stream and copies back):
+//   * device buffers are grow-only and owned by the handle, so steady-state
+//     calls allocate nothing;
+//   * the batch is cut into chunks that rotate over the handle's lanes
+//     (streams): chunk c's host->device copy overlaps chunk c-1's kernels and
+//     chunk c-2's device->host copy;
+//   * per chunk: reset counters, bucket by size class when n varies, run each
+//     class's kernel, copy lengths/words/counters back;
+//   * caller buffers in pinned memory are copied directly; pageable ones go
+//     through the lane's pinned staging buffers.
+#include <algorithm>
+#include <chrono>
+#include <climits>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "runtime.cuh"
+
+namespace sbfs {
+
+size_t cta_smem_bytes(int nb_max);
+size_t cta_queue_entries(int nb_max, int ctas);
+int cta_max_ctas_per_sm(int nb_max, int threads);
+cudaError_t launch_cta(int nb_max, int threads, int ctas, const Batch &b, uint64_t *queues,
+                       unsigned long long *ticket, cudaStream_t st);
+size_t hbm_ctl_bytes();
+int hbm_max_ctas_per_sm(int threads);
+cudaError_t launch_hbm(int threads, int ctas, const Batch &b, uint32_t *bitmap, uint64_t *queue,
+                       void *ctl, unsigned long long *ticket, cudaStream_t st);
+cudaError_t plan_autotune(sbfs_handle *h, Plan &plan);
+
+cudaError_t DevBuf::reserve(size_t want)
+{
+    if (want <= bytes && ptr) return cudaSuccess;
+    release();
+    size_t sz = std::max<size_t>(want, 256);
+    cudaError_t e = cudaMalloc(&ptr, sz);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        cudaGetLastError();
+        return e;
+    }
+    bytes = sz;
+    return cudaSuccess;
+}
+
+void DevBuf::release()
+{
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+cudaError_t HostBuf::reserve(size_t want)
+{
+    if (want <= bytes && ptr) return cudaSuccess;
+    release();
+    size_t sz = std::max<size_t>(want, 256);
+    cudaError_t e = cudaHostAlloc(&ptr, sz, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        cudaGetLastError();
+        return e;
+    }
+    bytes = sz;
+    return cudaSuccess;
+}
+
+void HostBuf::release()
+{
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+}  // namespace sbfs
+
+using namespace sbfs;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+constexpr int kLanes = 2;
+constexpr int64_t kDefaultChunk = 1 << 19;
+
+sbfs_status fail(sbfs_handle *h, sbfs_status st, const std::string &msg)
+{
+    if (h)
+        h->last_error = msg;
+    else
+        g_create_error = msg;
+    return st;
+}
+
+sbfs_status cuda_fail(sbfs_handle *h, cudaError_t e, const char *what)
+{
+    std::string msg = std::string(what) + ": " + cudaGetErrorString(e);
+    cudaGetLastError();
+    return fail(h, e == cudaErrorMemoryAllocation ? SBFS_ENOMEM : SBFS_ECUDA, msg);
+}
+
+#define CK(call, what)                                   \
+    do {                                                 \
+        cudaError_t _e = (call);                         \
+        if (_e != cudaSuccess) return cuda_fail(h, _e, what); \
+    } while (0)
+
+bool is_pinned(const void *p)
+{
+    if (!p) return true;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+struct Job {
+    const uint8_t *maps;     // device
+    int32_t lstride;
+    const uint8_t *ns;       // device or null
+    int32_t n_uniform;
+    int32_t max_n;           // largest n in the job (bounds buffer sizes)
+    int64_t count;
+    int32_t *len;            // device or null
+    uint64_t *words;         // device or null
+    int32_t word_stride;
+};
+
+int class_present_mask(const Job &j)
+{
+    if (!j.ns) return 1 << class_of_n(j.n_uniform);
+    int m = 0;
+    for (int c = 0; c < kNumClasses; ++c)
+        if (c == 0 || j.max_n > (c ? kClassMaxN[c - 1] : 0)) m |= 1 << c;
+    return m;
+}
+
+// Reserve the lane's work buffers for a job and enqueue its kernels on the lane's
+// stream.  Counters must already be reset.
+sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches,
+                            unsigned long long *ticket_override = nullptr)
+{
+    const Plan &P = h->plan;
+    cudaStream_t st = L.stream;
+    DevCounters *ctr = L.counters.as<DevCounters>();
+    Batch b{};
+    b.maps = j.maps;
+    b.lstride = j.lstride;
+    b.ns = j.ns;
+    b.n_uniform = j.n_uniform;
+    b.order = nullptr;
+    b.count = j.count;
+    b.range_dev = nullptr;
+    b.out_len = j.len;
+    b.out_words = j.words;
+    b.word_stride = j.word_stride;
+    b.slack = h->cfg.slack;
+    b.first_violation = &ctr->first_violation;
+    b.expanded = &ctr->expanded;
+    b.error = &ctr->error;
+
+    const int present = class_present_mask(j);
+    if (j.ns) {
+        CK(L.order.reserve((size_t)j.count * sizeof(int32_t)), "allocating order array");
+        // hist[K] | ranges[2K] | cursor[K]
+        CK(L.ranges.reserve(4 * kNumClasses * sizeof(unsigned long long)), "allocating class ranges");
+        unsigned long long *r = L.ranges.as<unsigned long long>();
+        ClassScratch sc{r, r + kNumClasses, r + 3 * kNumClasses, L.order.as<int32_t>()};
+        CK(launch_classify(j.ns, j.count, sc, h->sm_count, st), "launching size-class bucketing");
+        *launches += 3;
+        b.order = sc.order;
+    }
+    for (int c = 0; c < kNumClasses; ++c) {
+        if (!(present & (1 << c))) continue;
+        Batch bc = b;
+        if (j.ns) bc.range_dev = L.ranges.as<unsigned long long>() + kNumClasses + 2 * c;
+        unsigned long long *ticket = ticket_override ? ticket_override : &ctr->ticket[c];
+        if (c < 3) {
+            const PoolShape &s = P.pool[c];
+            CK(L.spill.reserve(pool_spill_words(s) * sizeof(uint32_t)), "allocating queue spill");
+            CK(launch_pool(s, bc, L.spill.as<uint32_t>(), ticket, st), "launching small-n kernel");
+        } else if (c == 3) {
+            const int nb = std::min(20, std::max(j.ns ? j.max_n : j.n_uniform, 17));
+            const int per_sm = cta_max_ctas_per_sm(nb, P.cta.threads);
+            if (per_sm < 1) return fail(h, SBFS_ECUDA, "class-3 kernel does not fit on an SM");
+            const int ctas = std::min(P.cta.ctas, per_sm * h->sm_count);
+            CK(L.cta_queue.reserve(cta_queue_entries(nb, ctas) * sizeof(uint64_t)), "allocating CTA queues");
+            CK(launch_cta(nb, P.cta.threads, ctas, bc, L.cta_queue.as<uint64_t>(), ticket, st),
+               "launching n<=20 kernel");
+        } else {
+            const int nb = std::min(28, std::max(j.ns ? j.max_n : j.n_uniform, 21));
+            const size_t bitmap_bytes = ((size_t)1 << nb) / 8;
+            CK(L.hbm_bitmap.reserve(bitmap_bytes + hbm_ctl_bytes()), "allocating HBM bitmap");
+            CK(L.hbm_queue.reserve(((size_t)1 << nb) * sizeof(uint64_t)), "allocating HBM queue");
+            const int per_sm = hbm_max_ctas_per_sm(P.hbm.threads);
+            if (per_sm < 1) return fail(h, SBFS_ECUDA, "HBM kernel does not fit on an SM");
+            const int ctas = std::min(P.hbm.ctas, per_sm * h->sm_count);
+            void *ctl = L.hbm_bitmap.as<char>() + bitmap_bytes;
+            CK(launch_hbm(P.hbm.threads, ctas, bc, L.hbm_bitmap.as<uint32_t>(), L.hbm_queue.as<uint64_t>(),
+                          ctl, ticket, st),
+               "launching n<=28 kernel");
+        }
+        *launches += 1;
+    }
+    return SBFS_OK;
+}
+
+sbfs_status ensure_plan(sbfs_handle *h)
+{
+    if (h->plan_ready) return SBFS_OK;
+    Plan &P = h->plan;
+    const int sms = h->sm_count;
+    const int defaults[3][4] = {
+        // slots, warps, queue_smem
+        {16, 8, 64, 0},
+        {8, 4, 256, 0},
+        {4, 2, 256, 0},
+    };
+    for (int c = 0; c < 3; ++c) {
+        // configured shapes apply to every small-n class whose shared memory they fit
+        PoolShape &s = P.pool[c];
+        s.nmax = kClassMaxN[c];
+        s.slots = h->cfg.slots_per_warp > 0 ? h->cfg.slots_per_warp : defaults[c][0];
+        s.warps = h->cfg.warps_per_cta > 0 ? h->cfg.warps_per_cta : defaults[c][1];
+        s.queue_smem = h->cfg.queue_smem > 0 ? h->cfg.queue_smem : defaults[c][2];
+        s.ctas = 1;
+        int per_sm = pool_max_ctas_per_sm(s);
+        if (per_sm < 1) {
+            s.slots = defaults[c][0];
+            s.warps = defaults[c][1];
+            s.queue_smem = defaults[c][2];
+            per_sm = pool_max_ctas_per_sm(s);
+        }
+        if (per_sm < 1) return fail(h, SBFS_EINVAL, "small-n kernel shape does not fit in shared memory");
+        s.ctas = per_sm * sms;
+    }
+    P.cta.threads = 512;
+    P.cta.ctas = sms * 4;
+    P.hbm.threads = 512;
+    P.hbm.ctas = sms * 4;
+    if (h->cfg.autotune) {
+        cudaError_t e = plan_autotune(h, P);
+        if (e != cudaSuccess) return cuda_fail(h, e, "autotuning kernel shapes");
+    }
+    h->plan_ready = true;
+    return SBFS_OK;
+}
+
+sbfs_status check_records(sbfs_handle *h, const uint8_t *maps, int32_t lstride, const uint8_t *ns,
+                          int32_t n_uniform, int64_t count, int32_t *max_n)
+{
+    if (count < 0) return fail(h, SBFS_EINVAL, "negative count");
+    if (count > 0 && !maps) return fail(h, SBFS_EINVAL, "maps is NULL");
+    if (lstride < 1 || lstride > 32) return fail(h, SBFS_EINVAL, "lstride must be in 1..32");
+    if (!ns) {
+        if (n_uniform < 1 || n_uniform > SBFS_MAX_N || n_uniform > lstride)
+            return fail(h, SBFS_EINVAL, "n_uniform must be in 1..min(28, lstride)");
+        *max_n = n_uniform;
+    } else {
+        int m = 0;
+        for (int64_t i = 0; i < count; ++i) m = std::max<int>(m, ns[i]);
+        *max_n = std::min(m, SBFS_MAX_N);
+    }
+    return SBFS_OK;
+}
+
+sbfs_status reset_counters(sbfs_handle *h, Lane &L)
+{
+    CK(L.counters.reserve(sizeof(DevCounters)), "allocating counters");
+    CK(cudaMemsetAsync(L.counters.ptr, 0, sizeof(DevCounters), L.stream), "resetting counters");
+    CK(cudaMemsetAsync(&L.counters.as<DevCounters>()->first_violation, 0xFF, sizeof(unsigned long long),
+                       L.stream),
+       "resetting counters");
+    return SBFS_OK;
+}
+
+struct Totals {
+    int64_t first_violation = -1;
+    int64_t expanded = 0;
+    int error = 0;
+    double kernel_ms = 0;
+};
+
+sbfs_status finish_lane(sbfs_handle *h, Lane &L, Totals &t)
+{
+    if (!L.busy) return SBFS_OK;
+    L.busy = false;
+    CK(cudaEventSynchronize(L.ev_done), "waiting for a chunk");
+    const DevCounters *c = L.h_counters.as<DevCounters>();
+    t.error |= c->error;
+    t.expanded += (int64_t)c->expanded;
+    if (c->first_violation != ULLONG_MAX) {
+        const int64_t g = L.begin + (int64_t)c->first_violation;
+        if (t.first_violation < 0 || g < t.first_violation) t.first_violation = g;
+    }
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, L.ev_k0, L.ev_k1) == cudaSuccess) t.kernel_ms += ms;
+    cudaGetLastError();
+    if (L.staged_out) {
+        if (L.user_len) std::memcpy(L.user_len + L.begin, L.h_len.ptr, (size_t)L.count * sizeof(int32_t));
+        if (L.user_words)
+            std::memcpy(L.user_words + (size_t)L.begin * L.word_stride, L.h_words.ptr,
+                        (size_t)L.count * L.word_stride * sizeof(uint64_t));
+    }
+    return SBFS_OK;
+}
+
+sbfs_status solve_host(sbfs_handle *h, const uint8_t *maps, int32_t lstride, const uint8_t *ns,
+                       int32_t n_uniform, int64_t count, int32_t *out_len, uint64_t *out_words,
+                       int32_t word_stride, int64_t *out_first_violation, sbfs_stats *stats, bool plain)
+{
+    if (!h) return fail(nullptr, SBFS_EINVAL, "handle is NULL");
+    std::lock_guard<std::mutex> lock(h->mu);
+    h->last_error.clear();
+    const auto t0 = std::chrono::steady_clock::now();
+    int32_t max_n = 0;
+    sbfs_status s = check_records(h, maps, lstride, ns, n_uniform, count, &max_n);
+    if (s) return s;
+    if (out_words && word_stride < 1) return fail(h, SBFS_EINVAL, "word_stride must be >= 1");
+    if (!out_len && out_words) return fail(h, SBFS_EINVAL, "words need out_len");
+    CK(cudaSetDevice(h->device), "selecting device");
+    if ((s = ensure_plan(h))) return s;
+
+    const int64_t chunk = plain ? std::max<int64_t>(count, 1)
+                                : (h->cfg.chunk > 0 ? h->cfg.chunk : kDefaultChunk);
+    const bool pin_in = is_pinned(maps) && is_pinned(ns);
+    const bool pin_out = is_pinned(out_len) && is_pinned(out_words);
+    const size_t rec = 2 * (size_t)lstride;
+    Totals tot;
+    int launches = 0;
+    int64_t h2d = 0, d2h = 0;
+    const int nlanes = plain ? 1 : (int)h->lanes.size();
+
+    for (int64_t begin = 0, ci = 0; begin < count; begin += chunk, ++ci) {
+        Lane &L = h->lanes[ci % nlanes];
+        if ((s = finish_lane(h, L, tot))) return s;
+        const int64_t cnt = std::min(chunk, count - begin);
+        CK(L.maps.reserve(cnt * rec), "allocating records");
+        if (ns) CK(L.ns.reserve(cnt), "allocating sizes");
+        if (out_len) CK(L.len.reserve(cnt * sizeof(int32_t)), "allocating lengths");
+        if (out_words) CK(L.words.reserve(cnt * word_stride * sizeof(uint64_t)), "allocating words");
+        CK(L.h_counters.reserve(sizeof(DevCounters)), "allocating pinned counters");
+        const uint8_t *src_maps = maps + begin * rec;
+        const uint8_t *src_ns = ns ? ns + begin : nullptr;
+        if (!pin_in) {
+            CK(L.h_maps.reserve(cnt * rec), "allocating pinned staging");
+            std::memcpy(L.h_maps.ptr, src_maps, cnt * rec);
+            src_maps = L.h_maps.as<uint8_t>();
+            if (ns) {
+                CK(L.h_ns.reserve(cnt), "allocating pinned staging");
+                std::memcpy(L.h_ns.ptr, src_ns, cnt);
+                src_ns = L.h_ns.as<uint8_t>();
+            }
+        }
+        CK(cudaMemcpyAsync(L.maps.ptr, src_maps, cnt * rec, cudaMemcpyHostToDevice, L.stream), "copying records");
+        h2d += cnt * rec;
+        if (ns) {
+            CK(cudaMemcpyAsync(L.ns.ptr, src_ns, cnt, cudaMemcpyHostToDevice, L.stream), "copying sizes");
+            h2d += cnt;
+        }
+        if ((s = reset_counters(h, L))) return s;
+        Job j{L.maps.as<uint8_t>(), lstride, ns ? L.ns.as<uint8_t>() : nullptr, n_uniform, max_n, cnt,
+              out_len ? L.len.as<int32_t>() : nullptr, out_words ? L.words.as<uint64_t>() : nullptr,
+              word_stride};
+        CK(cudaEventRecord(L.ev_k0, L.stream), "recording event");
+        if (!plain) {
+            if ((s = enqueue_kernels(h, L, j, &launches))) return s;
+        } else {
+            // one launch per automaton, same kernels, one-CTA grid
+            Plan saved = h->plan;
+            for (int c = 0; c < 3; ++c) h->plan.pool[c].ctas = 1;
+            h->plan.cta.ctas = 1;
+            h->plan.hbm.ctas = h->sm_count;   // the HBM kernel is grid-wide by construction
+            CK(L.escal.reserve((size_t)cnt * sizeof(unsigned long long)), "allocating tickets");
+            CK(cudaMemsetAsync(L.escal.ptr, 0, (size_t)cnt * sizeof(unsigned long long), L.stream),
+               "resetting tickets");
+            CK(cudaEventRecord(L.ev_k0, L.stream), "recording event");
+            for (int64_t i = 0; i < cnt; ++i) {
+                Job one = j;
+                one.maps = j.maps + i * rec;
+                one.ns = nullptr;
+                one.n_uniform = ns ? ns[begin + i] : n_uniform;
+                one.max_n = one.n_uniform;
+                one.count = 1;
+                one.len = j.len ? j.len + i : nullptr;
+                one.words = j.words ? j.words + i * word_stride : nullptr;
+                if (one.n_uniform < 1 || one.n_uniform > SBFS_MAX_N) {
+                    h->plan = saved;
+                    return fail(h, SBFS_EINVAL, "n out of range");
+                }
+                if ((s = enqueue_kernels(h, L, one, &launches, L.escal.as<unsigned long long>() + i))) {
+                    h->plan = saved;
+                    return s;
+                }
+            }
+            h->plan = saved;
+        }
+        CK(cudaEventRecord(L.ev_k1, L.stream), "recording event");
+        L.staged_out = !pin_out;
+        L.user_len = out_len;
+        L.user_words = out_words;
+        L.word_stride = word_stride;
+        if (out_len) {
+            void *dst = pin_out ? (void *)(out_len + begin) : nullptr;
+            if (!pin_out) {
+                CK(L.h_len.reserve(cnt * sizeof(int32_t)), "allocating pinned staging");
+                dst = L.h_len.ptr;
+            }
+            CK(cudaMemcpyAsync(dst, L.len.ptr, cnt * sizeof(int32_t), cudaMemcpyDeviceToHost, L.stream),
+               "copying lengths");
+            d2h += cnt * sizeof(int32_t);
+        }
+        if (out_words) {
+            const size_t wb = (size_t)cnt * word_stride * sizeof(uint64_t);
+            void *dst = pin_out ? (void *)(out_words + (size_t)begin * word_stride) : nullptr;
+            if (!pin_out) {
+                CK(L.h_words.reserve(wb), "allocating pinned staging");
+                dst = L.h_words.ptr;
+            }
+            CK(cudaMemcpyAsync(dst, L.words.ptr, wb, cudaMemcpyDeviceToHost, L.stream), "copying words");
+            d2h += wb;
+        }
+        CK(cudaMemcpyAsync(L.h_counters.ptr, L.counters.ptr, sizeof(DevCounters), cudaMemcpyDeviceToHost,
+                           L.stream),
+           "copying counters");
+        CK(cudaEventRecord(L.ev_done, L.stream), "recording event");
+        L.busy = true;
+        L.begin = begin;
+        L.count = cnt;
+    }
+    for (auto &L : h->lanes)
+        if ((s = finish_lane(h, L, tot))) return s;
+    if (out_first_violation) *out_first_violation = tot.first_violation;
+    if (stats) {
+        stats->automata = count;
+        stats->expanded = tot.expanded;
+        stats->synchronizing = 0;
+        if (out_len)
+            for (int64_t i = 0; i < count; ++i) stats->synchronizing += out_len[i] >= 0;
+        stats->h2d_bytes = h2d;
+        stats->d2h_bytes = d2h;
+        stats->launches = launches;
+        stats->classes = 0;
+        stats->kernel_ms = tot.kernel_ms;
+        stats->total_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    if (tot.error & kErrInvalid) return fail(h, SBFS_EINVAL, "malformed automaton: a state index >= n");
+    if (tot.error) return fail(h, SBFS_ETIMEOUT, "a device-side bounded wait ran out");
+    return SBFS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t sbfs_abi_version(void) { return SBFS_ABI_VERSION; }
+
+sbfs_status sbfs_config_default(sbfs_config *cfg)
+{
+    if (!cfg) return SBFS_EINVAL;
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->device = -1;
+    cfg->use_graph = 0;
+    cfg->autotune = 0;
+    return SBFS_OK;
+}
+
+const char *sbfs_status_string(sbfs_status s)
+{
+    switch (s) {
+    case SBFS_OK: return "ok";
+    case SBFS_EINVAL: return "invalid argument";
+    case SBFS_ENOMEM: return "out of memory";
+    case SBFS_ETIMEOUT: return "timed out";
+    case SBFS_ECUDA: return "CUDA error";
+    case SBFS_EBUSY: return "busy";
+    case SBFS_ENOTFOUND: return "not found";
+    case SBFS_ECANCELED: return "cancelled";
+    case SBFS_ESTOPPED: return "stopped";
+    }
+    return "unknown status";
+}
+
+sbfs_status sbfs_create(const sbfs_config *cfg, sbfs_handle **out)
+{
+    if (!out) return fail(nullptr, SBFS_EINVAL, "out is NULL");
+    *out = nullptr;
+    sbfs_config c;
+    sbfs_config_default(&c);
+    if (cfg) c = *cfg;
+    int dev = c.device;
+    cudaError_t e;
+    if (dev < 0) {
+        e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return cuda_fail(nullptr, e, "no CUDA device");
+    }
+    e = cudaSetDevice(dev);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "selecting device");
+    cudaDeviceProp prop;
+    e = cudaGetDeviceProperties(&prop, dev);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "reading device properties");
+    if (prop.major < 10) return fail(nullptr, SBFS_ECUDA, "libsbfs is built for sm_100a (B200)");
+    sbfs_handle *h = new (std::nothrow) sbfs_handle();
+    if (!h) return fail(nullptr, SBFS_ENOMEM, "allocating handle");
+    h->device = dev;
+    h->sm_count = prop.multiProcessorCount;
+    h->smem_optin = prop.sharedMemPerBlockOptin;
+    h->cfg = c;
+    h->lanes.resize(kLanes);
+    for (auto &L : h->lanes) {
+        if ((e = cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaEventCreate(&L.ev_k0)) != cudaSuccess || (e = cudaEventCreate(&L.ev_k1)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&L.ev_done, cudaEventDisableTiming)) != cudaSuccess) {
+            sbfs_destroy(h);
+            return cuda_fail(nullptr, e, "creating streams");
+        }
+    }
+    *out = h;
+    return SBFS_OK;
+}
+
+sbfs_status sbfs_destroy(sbfs_handle *h)
+{
+    if (!h) return SBFS_OK;
+    cudaSetDevice(h->device);
+    for (auto &L : h->lanes) {
+        if (L.stream) cudaStreamSynchronize(L.stream);
+        for (DevBuf *d : {&L.maps, &L.ns, &L.len, &L.words, &L.spill, &L.order, &L.counters, &L.ranges,
+                          &L.cta_queue, &L.hbm_bitmap, &L.hbm_queue, &L.escal})
+            d->release();
+        for (HostBuf *b : {&L.h_counters, &L.h_maps, &L.h_ns, &L.h_len, &L.h_words}) b->release();
+        if (L.ev_k0) cudaEventDestroy(L.ev_k0);
+        if (L.ev_k1) cudaEventDestroy(L.ev_k1);
+        if (L.ev_done) cudaEventDestroy(L.ev_done);
+        if (L.stream) cudaStreamDestroy(L.stream);
+    }
+    delete h;
+    return SBFS_OK;
+}
+
+const char *sbfs_last_error(const sbfs_handle *h)
+{
+    return h ? h->last_error.c_str() : g_create_error.c_str();
+}
+
+int32_t sbfs_best_parallelism(const sbfs_handle *h) { return h ? (int32_t)h->lanes.size() : 0; }
+
+int32_t sbfs_word_stride(int32_t max_n)
+{
+    if (max_n < 2) return 1;
+    const int64_t bits = (int64_t)(max_n - 1) * (max_n - 1);
+    return (int32_t)std::max<int64_t>(1, (bits + 63) / 64);
+}
+
+sbfs_status sbfs_solve_batch(sbfs_handle *h, const uint8_t *maps, int32_t lstride, const uint8_t *ns,
+                             int32_t n_uniform, int64_t count, int32_t *out_len, uint64_t *out_words,
+                             int32_t word_stride, int64_t *out_first_violation, sbfs_stats *stats)
+{
+    if (!out_len) return fail(h, SBFS_EINVAL, "out_len is NULL (use sbfs_verify_batch)");
+    return solve_host(h, maps, lstride, ns, n_uniform, count, out_len, out_words, word_stride,
+                      out_first_violation, stats, false);
+}
+
+sbfs_status sbfs_verify_batch(sbfs_handle *h, const uint8_t *maps, int32_t lstride, const uint8_t *ns,
+                              int32_t n_uniform, int64_t count, int32_t *out_len,
+                              int64_t *out_first_violation, sbfs_stats *stats)
+{
+    return solve_host(h, maps, lstride, ns, n_uniform, count, out_len, nullptr, 0, out_first_violation, stats,
+                      false);
+}
+
+sbfs_status sbfs_solve_plain(sbfs_handle *h, const uint8_t *maps, int32_t lstride, const uint8_t *ns,
+                             int32_t n_uniform, int64_t count, int32_t *out_len, uint64_t *out_words,
+                             int32_t word_stride, int64_t *out_first_violation, sbfs_stats *stats)
+{
+    if (!out_len) return fail(h, SBFS_EINVAL, "out_len is NULL");
+    return solve_host(h, maps, lstride, ns, n_uniform, count, out_len, out_words, word_stride,
+                      out_first_violation, stats, true);
+}
+
+sbfs_status sbfs_solve_batch_device(sbfs_handle *h, const uint8_t *d_maps, int32_t lstride,
+                                    const uint8_t *d_ns, int32_t n_uniform, int64_t count, int32_t *d_len,
+                                    uint64_t *d_words, int32_t word_stride, int64_t *d_first_violation,
+                                    void *stream, sbfs_stats *stats)
+{
+    (void)d_first_violation;
+    (void)stream;
+    (void)stats;
+    (void)d_maps;
+    (void)lstride;
+    (void)d_ns;
+    (void)n_uniform;
+    (void)count;
+    (void)d_len;
+    (void)d_words;
+    (void)word_stride;
+    return fail(h, SBFS_EINVAL, "not implemented yet");
+}
+
+}  // extern "C"

@@ -1,0 +1,95 @@
+// common.cuh -- shared definitions of the sbfs CUDA kernels and host code.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "sbfs.h"
+
+namespace sbfs {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+// Length codes written to out_len besides real lengths.
+constexpr int32_t kLenNonSync = -1;   // queue emptied without a singleton
+constexpr int32_t kLenInvalid = -2;   // malformed record (state >= n); host turns into EINVAL
+
+// Device error bits (one int per launch set, read back by the host).
+constexpr int kErrInvalid = 1;        // malformed automaton seen
+constexpr int kErrCapacity = 2;       // a queue or frontier exceeded its reserved space
+
+// Everything a BFS kernel needs to know about the batch.
+struct Batch {
+    const uint8_t *maps;        // records, 2*lstride bytes each
+    int32_t lstride;
+    const uint8_t *ns;          // per-automaton n or nullptr
+    int32_t n_uniform;
+    const int32_t *order;       // indices of the automata this launch handles, or nullptr = 0..count-1
+    int64_t count;              // entries in order (or automata when order == nullptr)
+    // When set, range_dev[0] is an offset into order and range_dev[1] the count
+    // (a size class produced on the device by the bucketing kernels).
+    const unsigned long long *range_dev;
+    int32_t *out_len;           // nullable (pure Verify)
+    uint64_t *out_words;        // nullable
+    int32_t word_stride;
+    int32_t slack;
+    unsigned long long *first_violation;   // atomicMin target, starts at ULLONG_MAX
+    unsigned long long *expanded;          // stats counter (nullable)
+    int *error;                            // error bits
+};
+
+__device__ __forceinline__ int automaton_n(const Batch &b, int64_t k)
+{
+    return b.ns ? (int)b.ns[k] : b.n_uniform;
+}
+
+// Resolves the launch's work list: count and the base of the order array.
+__device__ __forceinline__ void resolve_work(const Batch &b, int64_t &count, const int32_t *&order)
+{
+    if (b.range_dev) {
+        order = b.order + b.range_dev[0];
+        count = (int64_t)b.range_dev[1];
+    } else {
+        order = b.order;
+        count = b.count;
+    }
+}
+
+__device__ __forceinline__ int64_t automaton_at(const int32_t *order, int64_t pos)
+{
+    return order ? (int64_t)order[pos] : pos;
+}
+
+__device__ __forceinline__ int cerny_bound(int n, int slack)
+{
+    return (n - 1) * (n - 1) - slack;
+}
+
+__device__ __forceinline__ bool is_singleton(uint32_t s)
+{
+    return (s & (s - 1u)) == 0u;
+}
+
+__device__ __forceinline__ void record_result(const Batch &b, int64_t k, int n, int32_t len)
+{
+    if (b.out_len) b.out_len[k] = len;
+    if (len > cerny_bound(n, b.slack))
+        atomicMin(b.first_violation, (unsigned long long)k);
+}
+
+// Host-side launch helpers implemented in the kernel translation units.
+struct PoolShape {
+    int nmax;          // size class bound: 8, 12 or 16
+    int slots;         // automata in flight per warp
+    int warps;         // warps per CTA
+    int queue_smem;    // on-chip queue entries per automaton
+    int ctas;          // grid size (persistent)
+};
+
+size_t pool_smem_bytes(const PoolShape &s);
+size_t pool_spill_words(const PoolShape &s);   // uint32 spill words for the whole grid
+cudaError_t launch_pool(const PoolShape &s, const Batch &b, uint32_t *spill,
+                        unsigned long long *ticket, cudaStream_t st);
+int pool_max_ctas_per_sm(const PoolShape &s);
+
+}  // namespace sbfs

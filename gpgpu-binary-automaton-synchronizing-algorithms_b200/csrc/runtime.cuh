@@ -1,0 +1,87 @@
+// runtime.cuh -- host-side engine behind the C ABI: handle state, device
+// buffers, per-class launch planning.
+#pragma once
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "classes.cuh"
+#include "common.cuh"
+#include "sbfs.h"
+
+namespace sbfs {
+
+// Counters one launch sequence reads and writes on the device.
+struct DevCounters {
+    unsigned long long ticket[kNumClasses + 1];   // per-class work tickets (+ escalation list)
+    unsigned long long first_violation;
+    unsigned long long expanded;
+    unsigned long long escalated;                 // entries appended to the escalation list
+    int error;
+    int pad;
+};
+
+// Grow-only device allocation.
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t reserve(size_t want);
+    void release();
+    template <class T> T *as() const { return static_cast<T *>(ptr); }
+};
+
+// Grow-only pinned host allocation.
+struct HostBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t reserve(size_t want);
+    void release();
+    template <class T> T *as() const { return static_cast<T *>(ptr); }
+};
+
+// Parameters of the large-n kernels (classes 3 and 4).
+struct CtaShape {
+    int threads;    // threads per CTA
+    int ctas;       // grid size (persistent)
+};
+
+// One stream with everything one in-flight chunk needs.
+struct Lane {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr, ev_done = nullptr;
+    DevBuf maps, ns, len, words, spill, order, counters, ranges, cta_queue, hbm_bitmap, hbm_queue,
+        escal;
+    HostBuf h_counters;                        // pinned copy of DevCounters
+    HostBuf h_maps, h_ns, h_len, h_words;      // pinned staging for pageable callers
+    // chunk bookkeeping
+    bool busy = false;
+    int64_t begin = 0, count = 0;
+    bool staged_out = false;
+    int32_t *user_len = nullptr;
+    uint64_t *user_words = nullptr;
+    int32_t word_stride = 0;
+};
+
+struct Plan {
+    PoolShape pool[3];
+    CtaShape cta;
+    CtaShape hbm;
+};
+
+}  // namespace sbfs
+
+struct sbfs_handle {
+    int device = 0;
+    int sm_count = 0;
+    size_t smem_optin = 0;
+    sbfs_config cfg{};
+    std::string last_error;
+    std::mutex mu;
+    std::vector<sbfs::Lane> lanes;
+    sbfs::Plan plan{};
+    bool plan_ready = false;
+};

@@ -1,0 +1,184 @@
+"""Host-side mirror of the reference's solver plugin contract over the C ABI.
+
+``Engine`` owns one ``sbfs_handle`` (include/sbfs.h) and works on packed numpy
+records.  ``SlimGPUNative`` implements the reference interface
+``IComputable`` (GPGPU/Interfaces/IComputable.cs:11-20) on ``Problem`` /
+``ComputationResult`` objects, with the same argument meaning:
+
+  Compute(problems, problemsReadingIndex, computationResults,
+          resultsWritingIndex, problemCount, degreeOfParallelism) -> int
+  Verify(problems, problemsReadingIndex, problemCount, degreeOfParallelism) -> int
+  GetBestParallelism() -> int
+
+Both return the index of the first automaton whose shortest word is longer
+than (n-1)^2 (a counterexample to Cerny's conjecture), else -1.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _native
+from .problem import Problem, records_from_problems, RECORD_LSTRIDE
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def word_stride_for(max_n: int) -> int:
+    return max(1, ((max(max_n, 2) - 1) ** 2 + 63) // 64)
+
+
+class Engine:
+    """One native handle: streams, device buffers, kernel plan."""
+
+    def __init__(self, device: int = -1, slack: int = 0, autotune: bool = False, use_graph: bool = False,
+                 slots_per_warp: int = 0, warps_per_cta: int = 0, queue_smem: int = 0, chunk: int = 0,
+                 tune_cache: Optional[str] = None):
+        self.lib = _native.load()
+        cfg = _native.Config()
+        self.lib.sbfs_config_default(ctypes.byref(cfg))
+        cfg.device = device
+        cfg.slack = slack
+        cfg.autotune = int(autotune)
+        cfg.use_graph = int(use_graph)
+        cfg.slots_per_warp = slots_per_warp
+        cfg.warps_per_cta = warps_per_cta
+        cfg.queue_smem = queue_smem
+        cfg.chunk = chunk
+        self._tune_cache = tune_cache.encode() if tune_cache else None
+        cfg.tune_cache = self._tune_cache
+        h = ctypes.c_void_p()
+        st = self.lib.sbfs_create(ctypes.byref(cfg), ctypes.byref(h))
+        if st != 0:
+            msg = self.lib.sbfs_last_error(None)
+            raise _native.SbfsError(st, msg.decode() if msg else "")
+        self.handle = h
+        self.last_stats: Optional[dict] = None
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.sbfs_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def best_parallelism(self) -> int:
+        return int(self.lib.sbfs_best_parallelism(self.handle))
+
+    def _prep(self, recs, ns, n, lstride):
+        recs = np.ascontiguousarray(recs, dtype=np.uint8)
+        if recs.ndim != 2 or recs.shape[1] != 2 * lstride:
+            raise ValueError(f"records must have shape (count, {2 * lstride})")
+        ns_arr = None if ns is None else np.ascontiguousarray(ns, dtype=np.uint8)
+        if ns_arr is not None and ns_arr.shape[0] != recs.shape[0]:
+            raise ValueError("ns must have one entry per record")
+        max_n = int(ns_arr.max()) if (ns_arr is not None and ns_arr.size) else int(n)
+        return recs, ns_arr, max_n
+
+    def solve(self, recs, ns=None, n: int = 0, lstride: int = RECORD_LSTRIDE, words: bool = True,
+              word_stride: Optional[int] = None, plain: bool = False, out=None):
+        """Solve every automaton.  Returns dict(len, words, word_stride,
+        first_violation, stats).  ``out`` may pass preallocated (len, words)."""
+        recs, ns_arr, max_n = self._prep(recs, ns, n, lstride)
+        count = recs.shape[0]
+        ws = int(word_stride or word_stride_for(max_n))
+        if out is not None:
+            out_len, out_words = out
+        else:
+            out_len = np.empty(count, dtype=np.int32)
+            out_words = np.empty((count, ws), dtype=np.uint64) if words else None
+        fv = ctypes.c_int64(-1)
+        stats = _native.Stats()
+        fn = self.lib.sbfs_solve_plain if plain else self.lib.sbfs_solve_batch
+        st = fn(self.handle, _ptr(recs), lstride, _ptr(ns_arr), int(n), count, _ptr(out_len),
+                _ptr(out_words) if words else None, ws if words else 0, ctypes.byref(fv),
+                ctypes.byref(stats))
+        self.last_stats = stats.as_dict()
+        _native.check(self.handle, st)
+        return {"len": out_len, "words": out_words if words else None, "word_stride": ws,
+                "first_violation": fv.value, "stats": self.last_stats}
+
+    def verify(self, recs, ns=None, n: int = 0, lstride: int = RECORD_LSTRIDE, lengths: bool = True):
+        """Lengths only (IComputable.Verify); returns dict(len, first_violation, stats)."""
+        recs, ns_arr, _ = self._prep(recs, ns, n, lstride)
+        count = recs.shape[0]
+        out_len = np.empty(count, dtype=np.int32) if lengths else None
+        fv = ctypes.c_int64(-1)
+        stats = _native.Stats()
+        st = self.lib.sbfs_verify_batch(self.handle, _ptr(recs), lstride, _ptr(ns_arr), int(n), count,
+                                        _ptr(out_len), ctypes.byref(fv), ctypes.byref(stats))
+        self.last_stats = stats.as_dict()
+        _native.check(self.handle, st)
+        return {"len": out_len, "first_violation": fv.value, "stats": self.last_stats}
+
+
+@dataclass
+class ComputationResult:
+    """Mirror of GPGPU/Shared/ComputationResult.cs:9-20 (fields the path fills)."""
+
+    isSynchronizable: bool = False
+    shortestSynchronizingWord: Optional[List[bool]] = None
+    shortestSynchronizingWordLength: int = 0
+    size: int = 0
+    algorithmName: str = ""
+    computationType: str = "GPU"
+    discoveredVertices: int = 0
+    queueBreadth: int = 0
+
+
+def word_bits_to_bools(bits: np.ndarray, length: int) -> List[bool]:
+    """uint64 word bits -> the reference's bool[] (true = letter b, index 0 first)."""
+    return [bool((int(bits[k >> 6]) >> (k & 63)) & 1) for k in range(length)]
+
+
+class SlimGPUNative:
+    """IComputable (GPGPU/Interfaces/IComputable.cs:11-20) on the B200 engine."""
+
+    def __init__(self, engine: Optional[Engine] = None, **engine_kwargs):
+        self.engine = engine or Engine(**engine_kwargs)
+
+    def GetBestParallelism(self) -> int:  # IComputable.cs:19
+        return self.engine.best_parallelism()
+
+    def Compute(self, problemsToSolve: Sequence[Problem], problemsReadingIndex: int,
+                computationResults: Optional[list], resultsWritingIndex: int, problemCount: int,
+                degreeOfParallelism: int) -> int:  # IComputable.cs:14
+        if problemCount == 0:
+            return -1
+        probs = problemsToSolve[problemsReadingIndex:problemsReadingIndex + problemCount]
+        recs, ns = records_from_problems(probs)
+        if computationResults is None:
+            r = self.engine.verify(recs, ns=ns, lengths=False)
+            fv = r["first_violation"]
+            return -1 if fv < 0 else problemsReadingIndex + fv
+        r = self.engine.solve(recs, ns=ns, words=True)
+        for i, p in enumerate(probs):
+            L = int(r["len"][i])
+            res = ComputationResult(size=p.size, algorithmName=type(self).__name__)
+            if L >= 0:
+                res.isSynchronizable = True
+                res.shortestSynchronizingWordLength = L
+                res.shortestSynchronizingWord = word_bits_to_bools(r["words"][i], L)
+            computationResults[resultsWritingIndex + i] = res
+        fv = r["first_violation"]
+        return -1 if fv < 0 else resultsWritingIndex + fv
+
+    def Verify(self, problemsToSolve: Sequence[Problem], problemsReadingIndex: int, problemCount: int,
+               degreeOfParallelism: int) -> int:  # IComputable.cs:17
+        return self.Compute(problemsToSolve, problemsReadingIndex, None, -1, problemCount,
+                            degreeOfParallelism)

@@ -1,0 +1,159 @@
+/*
+ * sbfs.h -- C ABI of libsbfs.so, the B200 engine for exact shortest
+ * synchronizing words of binary automata (power-set BFS).
+ *
+ * This ABI is the native side of the reference's solver plugin contract,
+ * IComputable (GPGPU/Interfaces/IComputable.cs:11-20):
+ *
+ *   int Compute(Problem[] problemsToSolve, int problemsReadingIndex,
+ *               ComputationResult[] computationResults, int resultsWritingIndex,
+ *               int problemCount, int degreeOfParallelism);     -> sbfs_solve_batch
+ *   int Verify(Problem[] problemsToSolve, int problemsReadingIndex,
+ *              int problemCount, int degreeOfParallelism);      -> sbfs_verify_batch
+ *   int GetBestParallelism();                                    -> sbfs_best_parallelism
+ *
+ * and replaces the Alea GPU solver GPGPU/GPU/SlimGPUQueue.cs:23-208 (host side:
+ * allocate, copy, launch, copy back, Cerny check) and its kernel :210-407.
+ *
+ * Conventions
+ *  - Every call returns an sbfs_status; nothing throws or aborts.
+ *  - All host pointers are caller-owned and only read/written during the call
+ *    (the serving calls copy what they need before returning).
+ *  - One handle owns one CUDA stream set and its device buffers.  Calls on one
+ *    handle are serialised by the handle; different handles may be used from
+ *    different threads concurrently.
+ *
+ * Automaton records.  Automaton i occupies 2*lstride bytes at
+ * maps + i*2*lstride: a[j] = rec[j] and b[j] = rec[lstride + j] for j < n
+ * (Problem.stateTransitioningMatrixA/B, SharedDefinitions/Problem.cs:7-11).
+ * lstride = 32 is the general 64-byte record; lstride = n packs a uniform
+ * batch tightly.  n is per automaton (ns != NULL) or uniform (ns == NULL,
+ * n_uniform).  1 <= n <= 28 and n <= lstride.
+ *
+ * Results.  out_len[i] = shortest synchronizing word length, or -1 when the
+ * automaton is not synchronizing (ComputationResult.isSynchronizable /
+ * shortestSynchronizingWordLength, GPGPU/Shared/ComputationResult.cs:9-20).
+ * Words: word_stride uint64 per automaton, bit k (LSB first across the
+ * uint64s) = 1 when letter k is b; letter 0 is applied first (the bool[] word
+ * of GPGPU/CPU/CPU.cs:262-269, true = b).  Unused bits are zero.  A word longer
+ * than 64*word_stride is not stored (its bits are zero) but the length is.
+ * out_first_violation = smallest batch index whose length exceeds
+ * (n-1)^2 - slack (the Cerny check of every IComputable.Compute), else -1.
+ */
+#ifndef SBFS_H
+#define SBFS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define SBFS_API __declspec(dllexport)
+#else
+#define SBFS_API __attribute__((visibility("default")))
+#endif
+
+#define SBFS_MAX_N 28
+#define SBFS_ABI_VERSION 1
+
+typedef enum sbfs_status {
+    SBFS_OK = 0,
+    SBFS_EINVAL = 1,     /* bad argument or malformed automaton (state >= n)    */
+    SBFS_ENOMEM = 2,     /* device or pinned host allocation failed             */
+    SBFS_ETIMEOUT = 3,   /* a bounded wait ran out                              */
+    SBFS_ECUDA = 4,      /* a CUDA runtime call failed (see sbfs_last_error)    */
+    SBFS_EBUSY = 5,      /* admission refused for now / queue full              */
+    SBFS_ENOTFOUND = 6,  /* unknown request id                                  */
+    SBFS_ECANCELED = 7,  /* request cancelled before completion                 */
+    SBFS_ESTOPPED = 8    /* server stopped                                      */
+} sbfs_status;
+
+typedef struct sbfs_handle sbfs_handle;
+
+typedef struct sbfs_config {
+    int32_t device;            /* CUDA device ordinal; -1 = current device              */
+    int32_t slack;             /* violation when len > (n-1)^2 - slack; 0 = Cerny bound */
+    int32_t use_graph;         /* 1 = replay batches of an already-seen shape from CUDA graphs */
+    int32_t autotune;          /* 1 = measure kernel shapes on first use and cache them */
+    int32_t slots_per_warp;    /* small-n kernel: automata in flight per warp; 0 = auto */
+    int32_t warps_per_cta;     /* small-n kernel: warps per CTA; 0 = auto               */
+    int32_t queue_smem;        /* small-n kernel: on-chip queue entries per automaton; 0 = auto */
+    int32_t chunk;             /* host<->device pipeline chunk (automata); 0 = auto     */
+    const char *tune_cache;    /* autotuner cache file, or NULL for in-memory only      */
+} sbfs_config;
+
+typedef struct sbfs_stats {
+    int64_t automata;          /* automata solved by the call                           */
+    int64_t expanded;          /* subsets dequeued and expanded (sum over automata)     */
+    int64_t synchronizing;     /* automata with a synchronizing word                    */
+    int64_t h2d_bytes;         /* bytes copied host -> device                           */
+    int64_t d2h_bytes;         /* bytes copied device -> host                           */
+    int32_t launches;          /* kernels launched                                      */
+    int32_t classes;           /* size classes used (small / cta / hbm)                 */
+    double kernel_ms;          /* device time of the BFS kernels (CUDA events)          */
+    double total_ms;           /* wall time of the call                                 */
+} sbfs_stats;
+
+SBFS_API int32_t sbfs_abi_version(void);
+SBFS_API sbfs_status sbfs_config_default(sbfs_config *cfg);
+SBFS_API sbfs_status sbfs_create(const sbfs_config *cfg, sbfs_handle **out);
+SBFS_API sbfs_status sbfs_destroy(sbfs_handle *h);
+/* Message of the last failure on this handle ("" when none); h may be NULL
+ * for failures of sbfs_create.  Valid until the next call on the handle. */
+SBFS_API const char *sbfs_last_error(const sbfs_handle *h);
+SBFS_API const char *sbfs_status_string(sbfs_status s);
+
+/* IComputable.GetBestParallelism (IComputable.cs:19): the number of CUDA
+ * streams the batched path overlaps (SlimGPUQueue.cs:19 returns 1). */
+SBFS_API int32_t sbfs_best_parallelism(const sbfs_handle *h);
+
+/*
+ * IComputable.Compute (IComputable.cs:14) on host buffers.  Copies records in,
+ * solves every automaton, copies lengths (and words when out_words != NULL)
+ * out.  out_len may be NULL only together with out_words == NULL (then this is
+ * Verify).  word_stride is ignored when out_words == NULL.
+ */
+SBFS_API sbfs_status sbfs_solve_batch(sbfs_handle *h, const uint8_t *maps, int32_t lstride,
+                                      const uint8_t *ns, int32_t n_uniform, int64_t count,
+                                      int32_t *out_len, uint64_t *out_words, int32_t word_stride,
+                                      int64_t *out_first_violation, sbfs_stats *stats);
+
+/* IComputable.Verify (IComputable.cs:17): lengths only, no words; out_len may be
+ * NULL.  Returns the first violation through out_first_violation. */
+SBFS_API sbfs_status sbfs_verify_batch(sbfs_handle *h, const uint8_t *maps, int32_t lstride,
+                                       const uint8_t *ns, int32_t n_uniform, int64_t count,
+                                       int32_t *out_len, int64_t *out_first_violation,
+                                       sbfs_stats *stats);
+
+/* The plain form: one automaton per kernel launch, same kernel body, used as
+ * the per-automaton comparison point.  count automata are solved one by one. */
+SBFS_API sbfs_status sbfs_solve_plain(sbfs_handle *h, const uint8_t *maps, int32_t lstride,
+                                      const uint8_t *ns, int32_t n_uniform, int64_t count,
+                                      int32_t *out_len, uint64_t *out_words, int32_t word_stride,
+                                      int64_t *out_first_violation, sbfs_stats *stats);
+
+/*
+ * Device-buffer form of sbfs_solve_batch: every pointer is device memory and
+ * the work is enqueued on `stream` (a cudaStream_t; NULL = the handle's
+ * stream).  *d_first_violation is an int64 in device memory.  The call
+ * returns once the work is enqueued; stats (host, may be NULL) then carry
+ * launch counts only.
+ */
+SBFS_API sbfs_status sbfs_solve_batch_device(sbfs_handle *h, const uint8_t *d_maps, int32_t lstride,
+                                             const uint8_t *d_ns, int32_t n_uniform, int64_t count,
+                                             int32_t *d_len, uint64_t *d_words, int32_t word_stride,
+                                             int64_t *d_first_violation, void *stream,
+                                             sbfs_stats *stats);
+
+/* uint64 per automaton needed for words of automata with at most max_n states:
+ * ceil((max_n-1)^2 / 64), at least 1. */
+SBFS_API int32_t sbfs_word_stride(int32_t max_n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SBFS_H */

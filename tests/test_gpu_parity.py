@@ -1,0 +1,160 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle.
+
+Bar: every length and non-synchronizing flag bit-exact; every returned word
+replays to a singleton and has the returned length; the Cerny bound (n-1)^2 is
+checked per automaton (Verify.cs:12-62).  Sizes follow the benchmark
+configurations with seeded synthetic inputs.
+"""
+import numpy as np
+import pytest
+
+import sbfs
+from sbfs import problem as P
+
+pytestmark = pytest.mark.gpu
+
+
+def _check(oracle_mod, recs, r, ns=None, n=0, lstride=32, ref=None):
+    if ref is None:
+        ref = oracle_mod.solve(recs, ns=ns, n=n, lstride=lstride, words=False, threads=8)
+    np.testing.assert_array_equal(r["len"], ref["len"])
+    if r.get("words") is not None:
+        bad, ok = oracle_mod.replay(recs, r["len"], r["words"], ns=ns, n=n, lstride=lstride)
+        assert bad == 0, np.nonzero(ok != 3)[0][:10]
+    assert r["first_violation"] == ref["first_violation"] == -1
+    return ref
+
+
+def test_config1_plain_n8(engine, oracle_mod):
+    recs = P.uniform_maps(10_000, 8, 0x5EED + 0)
+    r = engine.solve(recs, n=8)
+    ref = _check(oracle_mod, recs, r, n=8)
+    assert (r["len"] > 49).sum() == 0
+    # the GPU finishes the step in which the first singleton appears, the
+    # sequential oracle stops at that singleton: never fewer expansions
+    assert r["stats"]["expanded"] >= ref["expanded"]
+
+
+def test_config2_n12_full_batch_and_sample(engine, oracle_mod):
+    recs = P.uniform_maps(1_000_000, 12, 0x5EED + 1)
+    r = engine.solve(recs, n=12)
+    sample = slice(0, None, 100)
+    ref_s = oracle_mod.solve(recs[sample], n=12, words=False)
+    np.testing.assert_array_equal(r["len"][sample], ref_s["len"])
+    _check(oracle_mod, recs, r, n=12)
+
+
+def test_tight_records_same_as_64_byte_records(engine):
+    recs = P.uniform_maps(50_000, 12, 42)
+    a = engine.solve(recs, n=12, words=False)
+    b = engine.solve(P.repack(recs, 32, 12), n=12, lstride=12, words=False)
+    np.testing.assert_array_equal(a["len"], b["len"])
+
+
+@pytest.mark.parametrize("n", [3, 5, 8, 9, 12, 13, 16, 17, 20, 21, 24])
+def test_cerny_known_answers(engine, n):
+    recs = np.stack([P.cerny_record(n)] * 3)
+    r = engine.solve(recs, n=n)
+    assert (r["len"] == (n - 1) ** 2).all()
+
+
+def test_reference_worst_case_letters(engine, oracle_mod):
+    probs = [P.generate_worst_case(n) for n in range(3, 14)]
+    recs, ns = P.records_from_problems(probs)
+    r = engine.solve(recs, ns=ns)
+    assert list(r["len"]) == [(n - 1) ** 2 for n in range(3, 14)]
+    bad, _ = oracle_mod.replay(recs, r["len"], r["words"], ns=ns)
+    assert bad == 0
+
+
+@pytest.mark.parametrize("n", [4, 6, 10, 14, 16, 18, 20])
+def test_uniform_random_each_class(engine, oracle_mod, n):
+    cnt = 20_000 if n <= 16 else 2_000
+    recs = P.uniform_maps(cnt, n, 1000 + n)
+    r = engine.solve(recs, n=n)
+    _check(oracle_mod, recs, r, n=n)
+
+
+def test_mixed_sizes_with_cerny(engine, oracle_mod):
+    cnt = 20_000
+    ns = P.uniform_sizes(cnt, 6, 20, 0x5EED + 2)
+    recs = P.uniform_maps(cnt, ns, 0x5EED + 2)
+    idx = np.arange(0, cnt, 100)  # 1% Cerny
+    for i in idx:
+        recs[i] = P.cerny_record(int(ns[i]))
+    r = engine.solve(recs, ns=ns)
+    _check(oracle_mod, recs, r, ns=ns)
+    np.testing.assert_array_equal(r["len"][idx], (ns[idx].astype(np.int32) - 1) ** 2)
+
+
+def test_alone_equals_in_the_mix(engine):
+    ns = P.uniform_sizes(3000, 6, 22, 11)
+    recs = P.uniform_maps(3000, ns, 12)
+    mix = engine.solve(recs, ns=ns)
+    for i in range(0, 3000, 211):
+        one = engine.solve(recs[i:i + 1], ns=ns[i:i + 1])
+        assert one["len"][0] == mix["len"][i]
+
+
+def test_plain_form_matches_batched(engine):
+    recs = P.uniform_maps(300, 12, 77)
+    a = engine.solve(recs, n=12)
+    b = engine.solve(recs, n=12, plain=True)
+    np.testing.assert_array_equal(a["len"], b["len"])
+
+
+def test_verify_mode_and_slack(oracle_mod):
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    recs = np.stack([P.uniform_maps(1, 9, 1)[0]] * 5 + [P.cerny_record(9)] + [P.uniform_maps(1, 9, 2)[0]])
+    with sbfs.Engine(slack=1) as eng:
+        v = eng.verify(recs, n=9)
+        assert v["first_violation"] == 5
+        assert v["len"][5] == 64
+    with sbfs.Engine() as eng:
+        assert eng.verify(recs, n=9, lengths=False)["first_violation"] == -1
+
+
+def test_pinned_and_pageable_buffers_agree(engine):
+    import torch
+    recs = P.uniform_maps(70_000, 12, 5)
+    a = engine.solve(recs, n=12)
+    pin = torch.from_numpy(recs).pin_memory()
+    out_len = torch.empty(recs.shape[0], dtype=torch.int32).pin_memory()
+    out_words = torch.empty((recs.shape[0], 2), dtype=torch.int64).pin_memory()
+    b = engine.solve(pin.numpy(), n=12, out=(out_len.numpy(), out_words.numpy().view(np.uint64)))
+    np.testing.assert_array_equal(a["len"], b["len"])
+    np.testing.assert_array_equal(a["words"], b["words"])
+
+
+def test_malformed_automaton_is_rejected(engine):
+    recs = P.uniform_maps(100, 8, 3)
+    recs[17, 2] = 8  # state 8 in an 8-state automaton
+    with pytest.raises(sbfs.SbfsError) as ei:
+        engine.solve(recs, n=8)
+    assert ei.value.status == 1
+    # the handle stays usable
+    good = engine.solve(P.uniform_maps(10, 8, 3), n=8)
+    assert good["len"].shape == (10,)
+
+
+def test_empty_batch(engine):
+    r = engine.solve(np.zeros((0, 64), dtype=np.uint8), n=8)
+    assert r["len"].shape == (0,) and r["first_violation"] == -1
+
+
+def test_icomputable_mirror(engine, oracle_mod):
+    probs = P.problems_from_records(P.uniform_maps(500, 10, 8), 10)
+    solver = sbfs.SlimGPUNative(engine=engine)
+    results = [None] * 510
+    assert solver.Compute(probs, 0, results, 10, 500, solver.GetBestParallelism()) == -1
+    recs, ns = P.records_from_problems(probs)
+    ref = oracle_mod.solve(recs, ns=ns, words=False)
+    for i in range(500):
+        res = results[10 + i]
+        assert res.isSynchronizable == (ref["len"][i] >= 0)
+        if res.isSynchronizable:
+            assert res.shortestSynchronizingWordLength == ref["len"][i]
+            assert len(res.shortestSynchronizingWord) == ref["len"][i]
+    assert solver.Verify(probs, 0, 500, 1) == -1
