@@ -145,7 +145,7 @@ int class_present_mask(const Job &j)
 
 // Reserve the lane's work buffers for a job and enqueue its kernels on the lane's
 // stream.  Counters must already be reset.
-sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches,
+sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches, bool plain = false,
                             unsigned long long *ticket_override = nullptr)
 {
     const Plan &P = h->plan;
@@ -183,7 +183,13 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
         Batch bc = b;
         if (j.ns) bc.range_dev = L.ranges.as<unsigned long long>() + kNumClasses + 2 * c;
         unsigned long long *ticket = ticket_override ? ticket_override : &ctr->ticket[c];
-        if (c < 3) {
+        if (c < 2 && !plain) {
+            const LaneShape &ls = P.lane[c];
+            CK(L.escal.reserve((size_t)std::max<int64_t>(j.count, 1) * sizeof(int32_t)), "allocating escalation list");
+            CK(launch_lane(ls.nmax, ls.warps, ls.ring, ls.refill_k, ls.ctas, bc, L.escal.as<int32_t>(),
+                           &ctr->escal_range[1], ticket, st),
+               "launching per-lane kernel");
+        } else if (c < 3) {
             const PoolShape &s = P.pool[c];
             CK(L.spill.reserve(pool_spill_words(s) * sizeof(uint32_t)), "allocating queue spill");
             CK(launch_pool(s, bc, L.spill.as<uint32_t>(), ticket, st), "launching small-n kernel");
@@ -208,6 +214,19 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
                           ctl, ticket, st),
                "launching n<=28 kernel");
         }
+        *launches += 1;
+    }
+    if (!plain && (present & 3)) {
+        // automata the per-lane kernel handed back (frontier wider than its ring,
+        // or a word longer than an entry carries) go through the pooled kernel
+        Batch be = b;
+        be.ns = j.ns;
+        be.order = L.escal.as<int32_t>();
+        be.range_dev = ctr->escal_range;
+        const PoolShape &s = P.pool[1];
+        CK(L.spill.reserve(pool_spill_words(s) * sizeof(uint32_t)), "allocating queue spill");
+        CK(launch_pool(s, be, L.spill.as<uint32_t>(), &ctr->ticket[kNumClasses], st),
+           "launching escalation kernel");
         *launches += 1;
     }
     return SBFS_OK;
@@ -241,6 +260,21 @@ sbfs_status ensure_plan(sbfs_handle *h)
         }
         if (per_sm < 1) return fail(h, SBFS_EINVAL, "small-n kernel shape does not fit in shared memory");
         s.ctas = per_sm * sms;
+    }
+    const int lane_defaults[2][4] = {
+        // warps, ring, refill_k
+        {8, 32, 8, 0},
+        {1, 128, 8, 0},
+    };
+    for (int c = 0; c < 2; ++c) {
+        LaneShape &ls = P.lane[c];
+        ls.nmax = kClassMaxN[c];
+        ls.warps = lane_defaults[c][0];
+        ls.ring = lane_defaults[c][1];
+        ls.refill_k = lane_defaults[c][2];
+        const int per_sm = lane_max_ctas_per_sm(ls.nmax, ls.warps, ls.ring);
+        if (per_sm < 1) return fail(h, SBFS_EINVAL, "per-lane kernel shape does not fit in shared memory");
+        ls.ctas = per_sm * sms;
     }
     P.cta.threads = 512;
     P.cta.ctas = sms * 4;
@@ -379,8 +413,8 @@ sbfs_status solve_host(sbfs_handle *h, const uint8_t *maps, int32_t lstride, con
             for (int c = 0; c < 3; ++c) h->plan.pool[c].ctas = 1;
             h->plan.cta.ctas = 1;
             h->plan.hbm.ctas = h->sm_count;   // the HBM kernel is grid-wide by construction
-            CK(L.escal.reserve((size_t)cnt * sizeof(unsigned long long)), "allocating tickets");
-            CK(cudaMemsetAsync(L.escal.ptr, 0, (size_t)cnt * sizeof(unsigned long long), L.stream),
+            CK(L.tickets.reserve((size_t)cnt * sizeof(unsigned long long)), "allocating tickets");
+            CK(cudaMemsetAsync(L.tickets.ptr, 0, (size_t)cnt * sizeof(unsigned long long), L.stream),
                "resetting tickets");
             CK(cudaEventRecord(L.ev_k0, L.stream), "recording event");
             for (int64_t i = 0; i < cnt; ++i) {
@@ -396,7 +430,7 @@ sbfs_status solve_host(sbfs_handle *h, const uint8_t *maps, int32_t lstride, con
                     h->plan = saved;
                     return fail(h, SBFS_EINVAL, "n out of range");
                 }
-                if ((s = enqueue_kernels(h, L, one, &launches, L.escal.as<unsigned long long>() + i))) {
+                if ((s = enqueue_kernels(h, L, one, &launches, true, L.tickets.as<unsigned long long>() + i))) {
                     h->plan = saved;
                     return s;
                 }
@@ -535,7 +569,7 @@ sbfs_status sbfs_destroy(sbfs_handle *h)
     for (auto &L : h->lanes) {
         if (L.stream) cudaStreamSynchronize(L.stream);
         for (DevBuf *d : {&L.maps, &L.ns, &L.len, &L.words, &L.spill, &L.order, &L.counters, &L.ranges,
-                          &L.cta_queue, &L.hbm_bitmap, &L.hbm_queue, &L.escal})
+                          &L.cta_queue, &L.hbm_bitmap, &L.hbm_queue, &L.escal, &L.tickets})
             d->release();
         for (HostBuf *b : {&L.h_counters, &L.h_maps, &L.h_ns, &L.h_len, &L.h_words}) b->release();
         if (L.ev_k0) cudaEventDestroy(L.ev_k0);

@@ -92,4 +92,10 @@ cudaError_t launch_pool(const PoolShape &s, const Batch &b, uint32_t *spill,
                         unsigned long long *ticket, cudaStream_t st);
 int pool_max_ctas_per_sm(const PoolShape &s);
 
+size_t lane_smem_bytes(int nmax, int warps, int ring);
+int lane_max_ctas_per_sm(int nmax, int warps, int ring);
+cudaError_t launch_lane(int nmax, int warps, int ring, int refill_k, int ctas, const Batch &b,
+                        int32_t *escal_list, unsigned long long *escal_count, unsigned long long *ticket,
+                        cudaStream_t st);
+
 }  // namespace sbfs

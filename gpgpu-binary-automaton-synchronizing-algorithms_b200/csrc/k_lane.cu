@@ -1,0 +1,292 @@
+// k_lane.cu -- power-set BFS with one automaton per lane (n <= 12).
+//
+// Each lane runs the sequential BFS of GPGPU/CPU/SlimCPU4bits.cs:214-306 on its
+// own automaton: pop a subset, look up both images in its nibble table
+// (entry = a-image << 16 | b-image, SlimCPU4bits.cs:122-206), test-and-set them
+// in its visited bitmap, append the new ones, advance the level when the
+// current level is used up (SlimCPUUntweaked.cs:126-130,160-164), stop at the
+// first singleton generated (:151-155).  All 32 lanes of a warp do this in
+// lockstep on 32 different automata.
+//
+// Shared memory is lane-interleaved: element e of lane l's bitmap, table and
+// queue lives at [e][l], so every lane-private access of a warp touches 32
+// different banks.  The queue is a ring of R entries holding only the live
+// frontier (current level remainder + next level); each entry carries the
+// letters of the word that reaches it (bit NMAX + d = letter d, 1 = b), so a
+// word needs no parent pointers or retained history.
+//
+// Two rare cases leave this kernel: a frontier wider than R, and a word longer
+// than 32 - NMAX letters.  Such an automaton is abandoned and appended to an
+// escalation list that the warp-pooled kernel (k_pool.cu) solves afterwards.
+//
+// Lanes that finish wait until `refill_k` lanes of the warp are idle; then the
+// warp writes their results and loads new automata for all of them in one
+// pass, so the per-automaton set-up (record load, table build, bitmap clear)
+// runs with many lanes active instead of one.
+#include "common.cuh"
+
+namespace sbfs {
+namespace {
+
+constexpr int kActive = 0, kDone = 1, kEscalate = 2, kIdle = 3;
+
+__host__ __device__ constexpr int low_bit4(int v)
+{
+    return (v & 1) ? 0 : (v & 2) ? 1 : (v & 4) ? 2 : 3;
+}
+
+template <int NMAX>
+struct LaneGeom {
+    static constexpr int kBitmapWords = (1 << NMAX) / 32;
+    static constexpr int kChunks = (NMAX + 3) / 4;
+    static constexpr int kTable = kChunks * 16;
+    static constexpr uint32_t kMask = (1u << NMAX) - 1u;
+    static constexpr int kWordMax = 32 - NMAX;   // letters an entry can carry
+};
+
+template <int NMAX>
+__global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, int32_t *escal_list,
+                                              unsigned long long *escal_count, unsigned long long *ticket)
+{
+    using G = LaneGeom<NMAX>;
+    constexpr int BW = G::kBitmapWords;
+    constexpr int T = G::kTable;
+    extern __shared__ __align__(16) uint32_t smem[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    uint32_t *base = smem + (size_t)warp * (BW + T + ring) * 32;
+    uint32_t *bm = base + lane;                  // bm[w * 32]
+    uint32_t *tb = base + BW * 32 + lane;        // tb[e * 32]
+    uint32_t *rq = base + (BW + T) * 32 + lane;  // rq[i * 32]
+    const uint32_t rmask = (uint32_t)ring - 1u;
+
+    int64_t count;
+    const int32_t *order;
+    resolve_work(b, count, order);
+    const bool words = b.out_words != nullptr;
+
+    int state = kIdle;
+    int64_t k = -1;
+    int n = 0;
+    uint32_t head = 0, tail = 0, lvl_end = 0, level = 0;
+    int32_t res_len = kLenNonSync;
+    uint32_t res_word = 0;
+    bool more = true;
+    unsigned long long expanded = 0;
+
+    while (true) {
+        // ---- phase: finish waiting lanes, load new automata -----------------
+        const unsigned not_active = __ballot_sync(kFull, state != kActive);
+        const unsigned waiting = __ballot_sync(kFull, state == kDone || state == kEscalate);
+        if (not_active == kFull || (__popc(not_active) >= refill_k && (more || waiting))) {
+            if (state == kDone) {
+                record_result(b, k, n, res_len);
+                if (b.out_words) {
+                    uint64_t *w = b.out_words + (size_t)k * (size_t)b.word_stride;
+                    w[0] = res_len > 0 ? (uint64_t)res_word : 0ull;
+                    for (int c = 1; c < b.word_stride; ++c) w[c] = 0ull;
+                }
+            }
+            const unsigned esc = __ballot_sync(kFull, state == kEscalate);
+            if (esc) {
+                unsigned long long pos = 0;
+                const int leader = __ffs(esc) - 1;
+                if (lane == leader) pos = atomicAdd(escal_count, (unsigned long long)__popc(esc));
+                pos = __shfl_sync(kFull, pos, leader);
+                if (state == kEscalate) escal_list[pos + __popc(esc & ((1u << lane) - 1u))] = (int32_t)k;
+            }
+            if (state != kActive) state = kIdle;
+            const unsigned idle = __ballot_sync(kFull, state == kIdle);
+            if (more && idle) {
+                unsigned long long got = 0;
+                const int leader = __ffs(idle) - 1;
+                if (lane == leader) got = atomicAdd(ticket, (unsigned long long)__popc(idle));
+                got = __shfl_sync(kFull, got, leader);
+                if (got + __popc(idle) >= (unsigned long long)count) more = false;
+                if (state == kIdle) {
+                    const unsigned long long pos = got + __popc(idle & ((1u << lane) - 1u));
+                    if (pos < (unsigned long long)count) {
+                        k = automaton_at(order, (int64_t)pos);
+                        n = automaton_n(b, k);
+                        state = kActive;
+                    }
+                }
+                bool bad = false;
+                // every lane that just received an automaton sets it up
+                const bool fresh = (state == kActive) && (idle & (1u << lane));
+                if (fresh) {
+                    if (n < 1 || n > NMAX || n > b.lstride) bad = true;
+                    const uint8_t *rec = b.maps + (size_t)k * 2u * (size_t)b.lstride;
+                    uint32_t aw[G::kChunks] = {}, bw[G::kChunks] = {};
+                    if (!bad) {
+                        if ((b.lstride & 3) == 0) {
+                            const uint32_t *ra = reinterpret_cast<const uint32_t *>(rec);
+                            const uint32_t *rb = reinterpret_cast<const uint32_t *>(rec + b.lstride);
+#pragma unroll
+                            for (int c = 0; c < G::kChunks; ++c) {
+                                aw[c] = 4 * c < n ? __ldg(ra + c) : 0u;
+                                bw[c] = 4 * c < n ? __ldg(rb + c) : 0u;
+                            }
+                        } else {
+#pragma unroll
+                            for (int c = 0; c < G::kChunks; ++c) {
+                                aw[c] = 0u;
+                                bw[c] = 0u;
+#pragma unroll
+                                for (int j = 0; j < 4; ++j) {
+                                    if (4 * c + j < n) {
+                                        aw[c] |= (uint32_t)__ldg(rec + 4 * c + j) << (8 * j);
+                                        bw[c] |= (uint32_t)__ldg(rec + b.lstride + 4 * c + j) << (8 * j);
+                                    }
+                                }
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int c = 0; c < G::kChunks; ++c) {
+                        uint32_t s[4];
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const int st = 4 * c + j;
+                            const uint32_t av = (aw[c] >> (8 * j)) & 0xFFu, bv = (bw[c] >> (8 * j)) & 0xFFu;
+                            if (bad || st >= n) {
+                                s[j] = 0u;
+                            } else {
+                                if (av >= (uint32_t)n || bv >= (uint32_t)n) bad = true;
+                                s[j] = (1u << ((av & 15u) + 16)) | (1u << (bv & 15u));
+                            }
+                        }
+                        // table[c*16 + v] = OR of s[j] over the set bits j of v
+                        uint32_t t[16];
+                        t[0] = 0u;
+#pragma unroll
+                        for (int v = 1; v < 16; ++v) t[v] = t[v & (v - 1)] | s[low_bit4(v)];
+#pragma unroll
+                        for (int v = 0; v < 16; ++v) tb[(c * 16 + v) * 32] = t[v];
+                    }
+                    if (bad) {
+                        if (b.out_len) b.out_len[k] = kLenInvalid;
+                        atomicOr(b.error, kErrInvalid);
+                        state = kIdle;
+                    } else {
+#pragma unroll 8
+                        for (int w = 0; w < BW; ++w) bm[w * 32] = 0u;
+                        const uint32_t full = (1u << n) - 1u;
+                        bm[(full >> 5) * 32] = 1u << (full & 31u);
+                        rq[0] = full;
+                        head = 0;
+                        tail = 1;
+                        lvl_end = 1;
+                        level = 0;
+                    }
+                }
+            }
+            if (__ballot_sync(kFull, state == kActive) == 0u) {
+                if (!more) break;
+                continue;
+            }
+        }
+
+        // ---- one expansion per active lane ----------------------------------
+        if (state == kActive) {
+            const uint32_t e = rq[(head & rmask) * 32];
+            ++head;
+            ++expanded;
+            const uint32_t x = e & G::kMask;
+            const uint32_t wbits = e >> NMAX;
+            uint32_t t = tb[(x & 15u) * 32];
+            if (G::kChunks > 1) t |= tb[(16 + ((x >> 4) & 15u)) * 32];
+            if (G::kChunks > 2) t |= tb[(32 + ((x >> 8) & 15u)) * 32];
+            const uint32_t ya = t >> 16, yb = t & 0xFFFFu;
+#pragma unroll
+            for (int letter = 0; letter < 2; ++letter) {
+                if (state != kActive) break;
+                const uint32_t y = letter ? yb : ya;
+                uint32_t *wp = bm + (y >> 5) * 32;
+                const uint32_t m = 1u << (y & 31u);
+                const uint32_t wv = *wp;
+                if (!(wv & m)) {
+                    if (is_singleton(y)) {
+                        state = kDone;
+                        res_len = (int32_t)level + 1;
+                        res_word = words ? (wbits | ((uint32_t)letter << level)) : 0u;
+                    } else if (tail - head >= (uint32_t)ring || (words && level >= (uint32_t)G::kWordMax)) {
+                        state = kEscalate;
+                    } else {
+                        *wp = wv | m;
+                        rq[(tail & rmask) * 32] =
+                            words ? (y | ((wbits | ((uint32_t)letter << level)) << NMAX)) : y;
+                        ++tail;
+                    }
+                }
+            }
+            if (state == kActive && head == lvl_end) {
+                if (tail == lvl_end) {
+                    state = kDone;
+                    res_len = kLenNonSync;
+                } else {
+                    lvl_end = tail;
+                    ++level;
+                }
+            }
+        }
+    }
+    for (int o = 16; o; o >>= 1) expanded += __shfl_down_sync(kFull, expanded, o);
+    if (lane == 0 && b.expanded) atomicAdd(b.expanded, expanded);
+}
+
+template <int NMAX>
+size_t smem_for(int warps, int ring)
+{
+    using G = LaneGeom<NMAX>;
+    return (size_t)warps * (G::kBitmapWords + G::kTable + ring) * 32 * sizeof(uint32_t);
+}
+
+template <int NMAX>
+const void *kptr() { return (const void *)k_lane<NMAX>; }
+
+}  // namespace
+
+size_t lane_smem_bytes(int nmax, int warps, int ring)
+{
+    return nmax <= 8 ? smem_for<8>(warps, ring) : smem_for<12>(warps, ring);
+}
+
+int lane_max_ctas_per_sm(int nmax, int warps, int ring)
+{
+    const void *k = nmax <= 8 ? kptr<8>() : kptr<12>();
+    const size_t smem = lane_smem_bytes(nmax, warps, ring);
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k, warps * 32, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return blocks;
+}
+
+cudaError_t launch_lane(int nmax, int warps, int ring, int refill_k, int ctas, const Batch &b,
+                        int32_t *escal_list, unsigned long long *escal_count, unsigned long long *ticket,
+                        cudaStream_t st)
+{
+    if ((ring & (ring - 1)) || ring < 8 || warps < 1 || warps > 8 || ctas < 1 || refill_k < 1 || refill_k > 32)
+        return cudaErrorInvalidValue;
+    const size_t smem = lane_smem_bytes(nmax, warps, ring);
+    if (nmax <= 8) {
+        cudaError_t e = cudaFuncSetAttribute(k_lane<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        k_lane<8><<<ctas, warps * 32, smem, st>>>(b, ring, refill_k, escal_list, escal_count, ticket);
+    } else if (nmax <= 12) {
+        cudaError_t e = cudaFuncSetAttribute(k_lane<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        k_lane<12><<<ctas, warps * 32, smem, st>>>(b, ring, refill_k, escal_list, escal_count, ticket);
+    } else {
+        return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace sbfs

@@ -20,7 +20,7 @@ struct DevCounters {
     unsigned long long ticket[kNumClasses + 1];   // per-class work tickets (+ escalation list)
     unsigned long long first_violation;
     unsigned long long expanded;
-    unsigned long long escalated;                 // entries appended to the escalation list
+    unsigned long long escal_range[2];            // {0, automata appended to the escalation list}
     int error;
     int pad;
 };
@@ -43,6 +43,15 @@ struct HostBuf {
     template <class T> T *as() const { return static_cast<T *>(ptr); }
 };
 
+// Parameters of the one-automaton-per-lane kernel (classes 0 and 1).
+struct LaneShape {
+    int nmax;       // 8 or 12
+    int warps;      // warps per CTA
+    int ring;       // on-chip frontier ring entries per lane (power of two)
+    int refill_k;   // idle lanes that trigger a refill pass
+    int ctas;       // grid size (persistent)
+};
+
 // Parameters of the large-n kernels (classes 3 and 4).
 struct CtaShape {
     int threads;    // threads per CTA
@@ -54,7 +63,7 @@ struct Lane {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr, ev_done = nullptr;
     DevBuf maps, ns, len, words, spill, order, counters, ranges, cta_queue, hbm_bitmap, hbm_queue,
-        escal;
+        escal, tickets;
     HostBuf h_counters;                        // pinned copy of DevCounters
     HostBuf h_maps, h_ns, h_len, h_words;      // pinned staging for pageable callers
     // chunk bookkeeping
@@ -67,6 +76,7 @@ struct Lane {
 };
 
 struct Plan {
+    LaneShape lane[2];
     PoolShape pool[3];
     CtaShape cta;
     CtaShape hbm;

@@ -116,7 +116,7 @@ def test_verify_mode_and_slack(oracle_mod):
         assert eng.verify(recs, n=9, lengths=False)["first_violation"] == -1
 
 
-def test_pinned_and_pageable_buffers_agree(engine):
+def test_pinned_and_pageable_buffers_agree(engine, oracle_mod):
     import torch
     recs = P.uniform_maps(70_000, 12, 5)
     a = engine.solve(recs, n=12)
@@ -125,7 +125,10 @@ def test_pinned_and_pageable_buffers_agree(engine):
     out_words = torch.empty((recs.shape[0], 2), dtype=torch.int64).pin_memory()
     b = engine.solve(pin.numpy(), n=12, out=(out_len.numpy(), out_words.numpy().view(np.uint64)))
     np.testing.assert_array_equal(a["len"], b["len"])
-    np.testing.assert_array_equal(a["words"], b["words"])
+    # a shortest word need not be unique; which one comes back may differ
+    # between runs, every one must replay to a singleton
+    for r in (a, b):
+        assert oracle_mod.replay(recs, r["len"], r["words"], n=12)[0] == 0
 
 
 def test_malformed_automaton_is_rejected(engine):
