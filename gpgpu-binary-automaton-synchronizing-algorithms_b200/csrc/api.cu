@@ -84,6 +84,11 @@ using namespace sbfs;
 
 namespace {
 
+__global__ void finalize_violation(const DevCounters *c, int64_t *out)
+{
+    *out = c->first_violation == ULLONG_MAX ? -1ll : (int64_t)c->first_violation;
+}
+
 thread_local std::string g_create_error;
 
 constexpr int kLanes = 2;
@@ -183,7 +188,7 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
         Batch bc = b;
         if (j.ns) bc.range_dev = L.ranges.as<unsigned long long>() + kNumClasses + 2 * c;
         unsigned long long *ticket = ticket_override ? ticket_override : &ctr->ticket[c];
-        if (c < 2 && !plain) {
+        if (c < 2 && !plain && h->cfg.small_kernel == 1) {
             const LaneShape &ls = P.lane[c];
             CK(L.escal.reserve((size_t)std::max<int64_t>(j.count, 1) * sizeof(int32_t)), "allocating escalation list");
             CK(launch_lane(ls.nmax, ls.warps, ls.ring, ls.refill_k, ls.ctas, bc, L.escal.as<int32_t>(),
@@ -216,7 +221,7 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
         }
         *launches += 1;
     }
-    if (!plain && (present & 3)) {
+    if (!plain && (present & 3) && h->cfg.small_kernel == 1) {
         // automata the per-lane kernel handed back (frontier wider than its ring,
         // or a word longer than an entry carries) go through the pooled kernel
         Batch be = b;
@@ -240,7 +245,7 @@ sbfs_status ensure_plan(sbfs_handle *h)
     const int defaults[3][4] = {
         // slots, warps, queue_smem
         {16, 8, 64, 0},
-        {8, 4, 256, 0},
+        {8, 2, 64, 0},
         {4, 2, 256, 0},
     };
     for (int c = 0; c < 3; ++c) {
@@ -269,9 +274,13 @@ sbfs_status ensure_plan(sbfs_handle *h)
     for (int c = 0; c < 2; ++c) {
         LaneShape &ls = P.lane[c];
         ls.nmax = kClassMaxN[c];
-        ls.warps = lane_defaults[c][0];
-        ls.ring = lane_defaults[c][1];
-        ls.refill_k = lane_defaults[c][2];
+        ls.warps = h->cfg.lane_warps > 0 ? h->cfg.lane_warps : lane_defaults[c][0];
+        ls.ring = h->cfg.lane_ring > 0 ? h->cfg.lane_ring : lane_defaults[c][1];
+        ls.refill_k = h->cfg.lane_refill > 0 ? h->cfg.lane_refill : lane_defaults[c][2];
+        if (lane_max_ctas_per_sm(ls.nmax, ls.warps, ls.ring) < 1) {
+            ls.warps = lane_defaults[c][0];
+            ls.ring = lane_defaults[c][1];
+        }
         const int per_sm = lane_max_ctas_per_sm(ls.nmax, ls.warps, ls.ring);
         if (per_sm < 1) return fail(h, SBFS_EINVAL, "per-lane kernel shape does not fit in shared memory");
         ls.ctas = per_sm * sms;
@@ -363,6 +372,7 @@ sbfs_status solve_host(sbfs_handle *h, const uint8_t *maps, int32_t lstride, con
     CK(cudaSetDevice(h->device), "selecting device");
     if ((s = ensure_plan(h))) return s;
 
+    if (h->device_pending) CK(cudaEventSynchronize(h->ev_device), "waiting for device work");
     const int64_t chunk = plain ? std::max<int64_t>(count, 1)
                                 : (h->cfg.chunk > 0 ? h->cfg.chunk : kDefaultChunk);
     const bool pin_in = is_pinned(maps) && is_pinned(ns);
@@ -550,6 +560,11 @@ sbfs_status sbfs_create(const sbfs_config *cfg, sbfs_handle **out)
     h->smem_optin = prop.sharedMemPerBlockOptin;
     h->cfg = c;
     h->lanes.resize(kLanes);
+    if ((e = cudaEventCreateWithFlags(&h->ev_device, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreate(&h->ev_dk0)) != cudaSuccess || (e = cudaEventCreate(&h->ev_dk1)) != cudaSuccess) {
+        sbfs_destroy(h);
+        return cuda_fail(nullptr, e, "creating events");
+    }
     for (auto &L : h->lanes) {
         if ((e = cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking)) != cudaSuccess ||
             (e = cudaEventCreate(&L.ev_k0)) != cudaSuccess || (e = cudaEventCreate(&L.ev_k1)) != cudaSuccess ||
@@ -577,6 +592,9 @@ sbfs_status sbfs_destroy(sbfs_handle *h)
         if (L.ev_done) cudaEventDestroy(L.ev_done);
         if (L.stream) cudaStreamDestroy(L.stream);
     }
+    if (h->ev_device) cudaEventDestroy(h->ev_device);
+    if (h->ev_dk0) cudaEventDestroy(h->ev_dk0);
+    if (h->ev_dk1) cudaEventDestroy(h->ev_dk1);
     delete h;
     return SBFS_OK;
 }
@@ -622,22 +640,151 @@ sbfs_status sbfs_solve_plain(sbfs_handle *h, const uint8_t *maps, int32_t lstrid
 }
 
 sbfs_status sbfs_solve_batch_device(sbfs_handle *h, const uint8_t *d_maps, int32_t lstride,
-                                    const uint8_t *d_ns, int32_t n_uniform, int64_t count, int32_t *d_len,
-                                    uint64_t *d_words, int32_t word_stride, int64_t *d_first_violation,
-                                    void *stream, sbfs_stats *stats)
+                                    const uint8_t *d_ns, int32_t n_uniform, int32_t max_n, int64_t count,
+                                    int32_t *d_len, uint64_t *d_words, int32_t word_stride,
+                                    int64_t *d_first_violation, void *stream)
 {
-    (void)d_first_violation;
-    (void)stream;
-    (void)stats;
-    (void)d_maps;
-    (void)lstride;
-    (void)d_ns;
-    (void)n_uniform;
-    (void)count;
-    (void)d_len;
-    (void)d_words;
-    (void)word_stride;
-    return fail(h, SBFS_EINVAL, "not implemented yet");
+    if (!h) return fail(nullptr, SBFS_EINVAL, "handle is NULL");
+    std::lock_guard<std::mutex> lock(h->mu);
+    h->last_error.clear();
+    if (count < 0 || (count > 0 && !d_maps)) return fail(h, SBFS_EINVAL, "bad records");
+    if (lstride < 1 || lstride > 32) return fail(h, SBFS_EINVAL, "lstride must be in 1..32");
+    if (!d_ns && (n_uniform < 1 || n_uniform > SBFS_MAX_N || n_uniform > lstride))
+        return fail(h, SBFS_EINVAL, "n_uniform must be in 1..min(28, lstride)");
+    if (d_words && word_stride < 1) return fail(h, SBFS_EINVAL, "word_stride must be >= 1");
+    if (!d_first_violation) return fail(h, SBFS_EINVAL, "d_first_violation is NULL");
+    CK(cudaSetDevice(h->device), "selecting device");
+    sbfs_status s = ensure_plan(h);
+    if (s) return s;
+    Lane &L = h->lanes[0];
+    if (L.busy) {
+        Totals t;
+        if ((s = finish_lane(h, L, t))) return s;
+    }
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : L.stream;
+    if (st != L.stream) {
+        // lane 0's buffers may still be read by earlier work on its own stream
+        CK(cudaEventRecord(L.ev_done, L.stream), "recording event");
+        CK(cudaStreamWaitEvent(st, L.ev_done, 0), "ordering streams");
+    }
+    CK(L.h_counters.reserve(sizeof(DevCounters)), "allocating pinned counters");
+    cudaStream_t saved = L.stream;
+    L.stream = st;
+    if ((s = reset_counters(h, L))) {
+        L.stream = saved;
+        return s;
+    }
+    Job j{d_maps, lstride, d_ns, n_uniform, d_ns ? (max_n > 0 ? std::min(max_n, SBFS_MAX_N) : SBFS_MAX_N) : n_uniform,
+          count, d_len, d_words, d_words ? word_stride : 0};
+    int launches = 0;
+    CK(cudaEventRecord(h->ev_dk0, st), "recording event");
+    if (count > 0) s = enqueue_kernels(h, L, j, &launches);
+    if (!s) {
+        launches += 1;
+        finalize_violation<<<1, 1, 0, st>>>(L.counters.as<DevCounters>(), d_first_violation);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) s = cuda_fail(h, e, "launching finalize");
+    }
+    L.stream = saved;
+    if (s) return s;
+    CK(cudaEventRecord(h->ev_dk1, st), "recording event");
+    CK(cudaMemcpyAsync(L.h_counters.ptr, L.counters.ptr, sizeof(DevCounters), cudaMemcpyDeviceToHost, st),
+       "copying counters");
+    CK(cudaEventRecord(h->ev_device, st), "recording event");
+    if (st != L.stream) CK(cudaStreamWaitEvent(L.stream, h->ev_device, 0), "ordering streams");
+    h->device_pending = true;
+    h->device_count = count;
+    h->device_launches = launches;
+    return SBFS_OK;
+}
+
+sbfs_status sbfs_device_wait(sbfs_handle *h, sbfs_stats *stats)
+{
+    if (!h) return fail(nullptr, SBFS_EINVAL, "handle is NULL");
+    std::lock_guard<std::mutex> lock(h->mu);
+    if (!h->device_pending) {
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        return SBFS_OK;
+    }
+    CK(cudaEventSynchronize(h->ev_device), "waiting for device work");
+    h->device_pending = false;
+    const DevCounters *c = h->lanes[0].h_counters.as<DevCounters>();
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->automata = h->device_count;
+        stats->expanded = (int64_t)c->expanded;
+        stats->launches = h->device_launches;
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, h->ev_dk0, h->ev_dk1) == cudaSuccess) stats->kernel_ms = ms;
+        cudaGetLastError();
+    }
+    if (c->error & kErrInvalid) return fail(h, SBFS_EINVAL, "malformed automaton: a state index >= n");
+    if (c->error) return fail(h, SBFS_ETIMEOUT, "a device-side bounded wait ran out");
+    return SBFS_OK;
+}
+
+int32_t sbfs_describe_plan(sbfs_handle *h, char *buf, int32_t len)
+{
+    if (!h) return 0;
+    std::lock_guard<std::mutex> lock(h->mu);
+    if (cudaSetDevice(h->device) != cudaSuccess || ensure_plan(h) != SBFS_OK) {
+        cudaGetLastError();
+        return 0;
+    }
+    const Plan &P = h->plan;
+    std::string js = "{\"small_kernel\":\"";
+    js += h->cfg.small_kernel == 1 ? "lane" : "pool";
+    js += "\",\"classes\":[";
+    char tmp[256];
+    for (int c = 0; c < 3; ++c) {
+        const bool lane = c < 2 && h->cfg.small_kernel == 1;
+        if (lane) {
+            const LaneShape &l = P.lane[c];
+            std::snprintf(tmp, sizeof tmp,
+                          "{\"class\":%d,\"max_n\":%d,\"kernel\":\"k_lane<%d>\",\"warps\":%d,\"ring\":%d,"
+                          "\"refill\":%d,\"ctas\":%d},",
+                          c, kClassMaxN[c], l.nmax, l.warps, l.ring, l.refill_k, l.ctas);
+        } else {
+            const PoolShape &q = P.pool[c];
+            std::snprintf(tmp, sizeof tmp,
+                          "{\"class\":%d,\"max_n\":%d,\"kernel\":\"k_pool<%d,%d>\",\"warps\":%d,"
+                          "\"queue_smem\":%d,\"ctas\":%d},",
+                          c, kClassMaxN[c], q.nmax, q.slots, q.warps, q.queue_smem, q.ctas);
+        }
+        js += tmp;
+    }
+    std::snprintf(tmp, sizeof tmp,
+                  "{\"class\":3,\"max_n\":20,\"kernel\":\"k_cta\",\"threads\":%d,\"ctas\":%d},"
+                  "{\"class\":4,\"max_n\":28,\"kernel\":\"k_hbm\",\"threads\":%d,\"ctas\":%d}]}",
+                  P.cta.threads, P.cta.ctas, P.hbm.threads, P.hbm.ctas);
+    js += tmp;
+    if (buf && len > 0) {
+        std::strncpy(buf, js.c_str(), (size_t)len - 1);
+        buf[len - 1] = '\0';
+    }
+    return (int32_t)js.size() + 1;
+}
+
+sbfs_status sbfs_host_alloc(size_t bytes, void **out)
+{
+    if (!out) return SBFS_EINVAL;
+    *out = nullptr;
+    cudaError_t e = cudaHostAlloc(out, bytes ? bytes : 1, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *out = nullptr;
+        return SBFS_ENOMEM;
+    }
+    return SBFS_OK;
+}
+
+sbfs_status sbfs_host_free(void *p)
+{
+    if (p && cudaFreeHost(p) != cudaSuccess) {
+        cudaGetLastError();
+        return SBFS_EINVAL;
+    }
+    return SBFS_OK;
 }
 
 }  // extern "C"

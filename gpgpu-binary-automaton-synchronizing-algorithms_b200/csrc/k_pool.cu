@@ -338,6 +338,7 @@ cudaError_t launch_n(const PoolShape &s, const Batch &b, uint32_t *spill,
     case 4: return launch_t<NMAX, 4>(s, b, spill, ticket, st);
     case 8: return launch_t<NMAX, 8>(s, b, spill, ticket, st);
     case 16: return launch_t<NMAX, 16>(s, b, spill, ticket, st);
+    case 32: return launch_t<NMAX, 32>(s, b, spill, ticket, st);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -349,6 +350,7 @@ const void *kernel_ptr(int slots)
     case 4: return (const void *)k_pool<NMAX, 4>;
     case 8: return (const void *)k_pool<NMAX, 8>;
     case 16: return (const void *)k_pool<NMAX, 16>;
+    case 32: return (const void *)k_pool<NMAX, 32>;
     default: return nullptr;
     }
 }

@@ -94,4 +94,10 @@ struct sbfs_handle {
     std::vector<sbfs::Lane> lanes;
     sbfs::Plan plan{};
     bool plan_ready = false;
+    // last sbfs_solve_batch_device call: lane 0's buffers are in use until ev_device
+    cudaEvent_t ev_device = nullptr;
+    bool device_pending = false;
+    int64_t device_count = 0;
+    int device_launches = 0;
+    cudaEvent_t ev_dk0 = nullptr, ev_dk1 = nullptr;
 };

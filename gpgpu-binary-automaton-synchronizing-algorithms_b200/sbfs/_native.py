@@ -17,7 +17,8 @@ LIB_PATH = os.path.join(HERE, "_lib", "libsbfs.so")
 EXPORTS = [
     "sbfs_abi_version", "sbfs_config_default", "sbfs_create", "sbfs_destroy", "sbfs_last_error",
     "sbfs_status_string", "sbfs_best_parallelism", "sbfs_solve_batch", "sbfs_verify_batch",
-    "sbfs_solve_plain", "sbfs_solve_batch_device", "sbfs_word_stride",
+    "sbfs_solve_plain", "sbfs_solve_batch_device", "sbfs_device_wait", "sbfs_host_alloc",
+    "sbfs_host_free", "sbfs_word_stride", "sbfs_describe_plan",
 ]
 
 STATUS = {0: "SBFS_OK", 1: "SBFS_EINVAL", 2: "SBFS_ENOMEM", 3: "SBFS_ETIMEOUT", 4: "SBFS_ECUDA",
@@ -45,6 +46,10 @@ class Config(ctypes.Structure):
         ("warps_per_cta", ctypes.c_int32),
         ("queue_smem", ctypes.c_int32),
         ("chunk", ctypes.c_int32),
+        ("small_kernel", ctypes.c_int32),
+        ("lane_ring", ctypes.c_int32),
+        ("lane_refill", ctypes.c_int32),
+        ("lane_warps", ctypes.c_int32),
         ("tune_cache", ctypes.c_char_p),
     ]
 
@@ -103,8 +108,16 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         getattr(L, name).restype = ctypes.c_int
     L.sbfs_verify_batch.argtypes = [P, P, i32, P, i32, i64, P, ctypes.POINTER(i64), ctypes.POINTER(Stats)]
     L.sbfs_verify_batch.restype = ctypes.c_int
-    L.sbfs_solve_batch_device.argtypes = [P, P, i32, P, i32, i64, P, P, i32, P, P, ctypes.POINTER(Stats)]
+    L.sbfs_solve_batch_device.argtypes = [P, P, i32, P, i32, i32, i64, P, P, i32, P, P]
     L.sbfs_solve_batch_device.restype = ctypes.c_int
+    L.sbfs_device_wait.argtypes = [P, ctypes.POINTER(Stats)]
+    L.sbfs_device_wait.restype = ctypes.c_int
+    L.sbfs_host_alloc.argtypes = [ctypes.c_size_t, ctypes.POINTER(P)]
+    L.sbfs_host_alloc.restype = ctypes.c_int
+    L.sbfs_describe_plan.argtypes = [P, ctypes.c_char_p, i32]
+    L.sbfs_describe_plan.restype = i32
+    L.sbfs_host_free.argtypes = [P]
+    L.sbfs_host_free.restype = ctypes.c_int
     _lib = L
     return L
 

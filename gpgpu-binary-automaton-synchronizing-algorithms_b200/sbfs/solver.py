@@ -38,6 +38,7 @@ class Engine:
 
     def __init__(self, device: int = -1, slack: int = 0, autotune: bool = False, use_graph: bool = False,
                  slots_per_warp: int = 0, warps_per_cta: int = 0, queue_smem: int = 0, chunk: int = 0,
+                 small_kernel: int = 0, lane_ring: int = 0, lane_refill: int = 0, lane_warps: int = 0,
                  tune_cache: Optional[str] = None):
         self.lib = _native.load()
         cfg = _native.Config()
@@ -50,6 +51,10 @@ class Engine:
         cfg.warps_per_cta = warps_per_cta
         cfg.queue_smem = queue_smem
         cfg.chunk = chunk
+        cfg.small_kernel = small_kernel
+        cfg.lane_ring = lane_ring
+        cfg.lane_refill = lane_refill
+        cfg.lane_warps = lane_warps
         self._tune_cache = tune_cache.encode() if tune_cache else None
         cfg.tune_cache = self._tune_cache
         h = ctypes.c_void_p()
@@ -76,6 +81,14 @@ class Engine:
 
     def __exit__(self, *exc):
         self.close()
+
+    def plan(self) -> dict:
+        """Kernel and shape per size class, as the native plan describes it."""
+        import json
+        need = self.lib.sbfs_describe_plan(self.handle, None, 0)
+        buf = ctypes.create_string_buffer(max(need, 1))
+        self.lib.sbfs_describe_plan(self.handle, buf, len(buf))
+        return json.loads(buf.value.decode()) if buf.value else {}
 
     def best_parallelism(self) -> int:
         return int(self.lib.sbfs_best_parallelism(self.handle))
@@ -112,6 +125,30 @@ class Engine:
         _native.check(self.handle, st)
         return {"len": out_len, "words": out_words if words else None, "word_stride": ws,
                 "first_violation": fv.value, "stats": self.last_stats}
+
+    def solve_device(self, d_maps, lstride: int, count: int, n: int = 0, d_ns=None, max_n: int = 0,
+                     d_len=None, d_words=None, word_stride: int = 0, d_first_violation=None,
+                     stream=None):
+        """Enqueue a solve on device buffers (torch tensors or raw device
+        addresses); returns immediately.  Call ``wait_device`` for status."""
+        def addr(x):
+            if x is None:
+                return None
+            return ctypes.c_void_p(x.data_ptr() if hasattr(x, "data_ptr") else int(x))
+        st_ptr = None
+        if stream is not None:
+            st_ptr = ctypes.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+        st = self.lib.sbfs_solve_batch_device(self.handle, addr(d_maps), lstride, addr(d_ns), int(n),
+                                              int(max_n), int(count), addr(d_len), addr(d_words),
+                                              int(word_stride), addr(d_first_violation), st_ptr)
+        _native.check(self.handle, st)
+
+    def wait_device(self) -> dict:
+        stats = _native.Stats()
+        st = self.lib.sbfs_device_wait(self.handle, ctypes.byref(stats))
+        self.last_stats = stats.as_dict()
+        _native.check(self.handle, st)
+        return self.last_stats
 
     def verify(self, recs, ns=None, n: int = 0, lstride: int = RECORD_LSTRIDE, lengths: bool = True):
         """Lengths only (IComputable.Verify); returns dict(len, first_violation, stats)."""

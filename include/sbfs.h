@@ -82,6 +82,10 @@ typedef struct sbfs_config {
     int32_t warps_per_cta;     /* small-n kernel: warps per CTA; 0 = auto               */
     int32_t queue_smem;        /* small-n kernel: on-chip queue entries per automaton; 0 = auto */
     int32_t chunk;             /* host<->device pipeline chunk (automata); 0 = auto     */
+    int32_t small_kernel;      /* n <= 12: 0 = auto, 1 = one automaton per lane, 2 = warp-pooled */
+    int32_t lane_ring;         /* per-lane kernel: on-chip frontier entries (power of 2); 0 = auto */
+    int32_t lane_refill;       /* per-lane kernel: idle lanes that trigger a refill; 0 = auto */
+    int32_t lane_warps;        /* per-lane kernel: warps per CTA; 0 = auto              */
     const char *tune_cache;    /* autotuner cache file, or NULL for in-memory only      */
 } sbfs_config;
 
@@ -136,17 +140,32 @@ SBFS_API sbfs_status sbfs_solve_plain(sbfs_handle *h, const uint8_t *maps, int32
                                       int64_t *out_first_violation, sbfs_stats *stats);
 
 /*
- * Device-buffer form of sbfs_solve_batch: every pointer is device memory and
- * the work is enqueued on `stream` (a cudaStream_t; NULL = the handle's
- * stream).  *d_first_violation is an int64 in device memory.  The call
- * returns once the work is enqueued; stats (host, may be NULL) then carry
- * launch counts only.
+ * Device-buffer form of sbfs_solve_batch: maps, ns, len and words are device
+ * memory and the work is enqueued on `stream` (a cudaStream_t; NULL = the
+ * handle's first stream).  *d_first_violation is an int64 in device memory
+ * (-1 = none).  max_n bounds the sizes in d_ns (0 = 28); it sizes the
+ * large-n buffers without reading d_ns back.  The call returns once the work
+ * is enqueued; sbfs_device_wait reports its errors and statistics.
  */
 SBFS_API sbfs_status sbfs_solve_batch_device(sbfs_handle *h, const uint8_t *d_maps, int32_t lstride,
-                                             const uint8_t *d_ns, int32_t n_uniform, int64_t count,
-                                             int32_t *d_len, uint64_t *d_words, int32_t word_stride,
-                                             int64_t *d_first_violation, void *stream,
-                                             sbfs_stats *stats);
+                                             const uint8_t *d_ns, int32_t n_uniform, int32_t max_n,
+                                             int64_t count, int32_t *d_len, uint64_t *d_words,
+                                             int32_t word_stride, int64_t *d_first_violation,
+                                             void *stream);
+
+/* Waits for the last sbfs_solve_batch_device call of this handle and reports
+ * its status (SBFS_EINVAL for a malformed automaton) and statistics. */
+SBFS_API sbfs_status sbfs_device_wait(sbfs_handle *h, sbfs_stats *stats);
+
+/* Pinned host memory for callers that want the copy-overlapped path without
+ * their own CUDA dependency (the C# shim uses it for its staging arrays). */
+SBFS_API sbfs_status sbfs_host_alloc(size_t bytes, void **out);
+SBFS_API sbfs_status sbfs_host_free(void *p);
+
+/* JSON description of the kernel plan the handle uses (kernel and shape per
+ * size class), written to buf (NUL-terminated, truncated to len).  Returns
+ * the full length needed. */
+SBFS_API int32_t sbfs_describe_plan(sbfs_handle *h, char *buf, int32_t len);
 
 /* uint64 per automaton needed for words of automata with at most max_n states:
  * ceil((max_n-1)^2 / 64), at least 1. */

@@ -161,3 +161,29 @@ def test_icomputable_mirror(engine, oracle_mod):
             assert res.shortestSynchronizingWordLength == ref["len"][i]
             assert len(res.shortestSynchronizingWord) == ref["len"][i]
     assert solver.Verify(probs, 0, 500, 1) == -1
+
+
+def test_device_buffer_path(engine, oracle_mod):
+    import torch
+    ns = P.uniform_sizes(30_000, 3, 20, 21)
+    recs = P.uniform_maps(30_000, ns, 22)
+    dev = torch.device("cuda", 0)
+    d_maps = torch.from_numpy(recs).to(dev)
+    d_ns = torch.from_numpy(ns).to(dev)
+    d_len = torch.empty(len(ns), dtype=torch.int32, device=dev)
+    d_words = torch.empty((len(ns), 6), dtype=torch.int64, device=dev)
+    d_fv = torch.empty(1, dtype=torch.int64, device=dev)
+    s = torch.cuda.Stream()
+    engine.solve_device(d_maps, 32, len(ns), d_ns=d_ns, max_n=20, d_len=d_len, d_words=d_words,
+                        word_stride=6, d_first_violation=d_fv, stream=s)
+    st = engine.wait_device()
+    assert st["automata"] == len(ns) and st["launches"] >= 3
+    lens = d_len.cpu().numpy()
+    ref = oracle_mod.solve(recs, ns=ns, words=False, threads=8)
+    np.testing.assert_array_equal(lens, ref["len"])
+    assert int(d_fv.item()) == -1
+    words = d_words.cpu().numpy().view(np.uint64)
+    assert oracle_mod.replay(recs, lens, words, ns=ns)[0] == 0
+    # the host path on the same handle afterwards still agrees
+    host = engine.solve(recs, ns=ns)
+    np.testing.assert_array_equal(host["len"], lens)
