@@ -266,7 +266,10 @@ def run_sbfs(args):
         return float(t.item())
 
     # ---- device-resident leg ------------------------------------------------
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the events, the L2 flush and the library's kernels all
+    # go on it (the legacy default stream would hand the library a NULL stream)
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
     d_maps = torch.from_numpy(wl["recs"]).to(dev)
     d_ns = torch.from_numpy(wl["ns"]).to(dev) if wl["ns"] is not None else None
     d_len = torch.empty(count, dtype=torch.int32, device=dev)

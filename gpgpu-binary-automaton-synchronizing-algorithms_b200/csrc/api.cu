@@ -91,8 +91,8 @@ __global__ void finalize_violation(const DevCounters *c, int64_t *out)
 
 thread_local std::string g_create_error;
 
-constexpr int kLanes = 2;
-constexpr int64_t kDefaultChunk = 1 << 19;
+constexpr int kDefaultLanes = 4;
+constexpr int64_t kDefaultChunk = 1 << 18;
 
 sbfs_status fail(sbfs_handle *h, sbfs_status st, const std::string &msg)
 {
@@ -188,7 +188,7 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
         Batch bc = b;
         if (j.ns) bc.range_dev = L.ranges.as<unsigned long long>() + kNumClasses + 2 * c;
         unsigned long long *ticket = ticket_override ? ticket_override : &ctr->ticket[c];
-        if (c < 2 && !plain && h->cfg.small_kernel == 1) {
+        if (c < 2 && !plain && h->cfg.small_kernel != 2) {
             const LaneShape &ls = P.lane[c];
             CK(L.escal.reserve((size_t)std::max<int64_t>(j.count, 1) * sizeof(int32_t)), "allocating escalation list");
             CK(launch_lane(ls.nmax, ls.warps, ls.ring, ls.refill_k, ls.ctas, bc, L.escal.as<int32_t>(),
@@ -221,7 +221,7 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
         }
         *launches += 1;
     }
-    if (!plain && (present & 3) && h->cfg.small_kernel == 1) {
+    if (!plain && (present & 3) && h->cfg.small_kernel != 2) {
         // automata the per-lane kernel handed back (frontier wider than its ring,
         // or a word longer than an entry carries) go through the pooled kernel
         Batch be = b;
@@ -268,8 +268,8 @@ sbfs_status ensure_plan(sbfs_handle *h)
     }
     const int lane_defaults[2][4] = {
         // warps, ring, refill_k
-        {8, 32, 8, 0},
-        {1, 128, 8, 0},
+        {4, 32, 16, 0},
+        {1, 32, 16, 0},
     };
     for (int c = 0; c < 2; ++c) {
         LaneShape &ls = P.lane[c];
@@ -559,7 +559,7 @@ sbfs_status sbfs_create(const sbfs_config *cfg, sbfs_handle **out)
     h->sm_count = prop.multiProcessorCount;
     h->smem_optin = prop.sharedMemPerBlockOptin;
     h->cfg = c;
-    h->lanes.resize(kLanes);
+    h->lanes.resize(c.streams > 0 ? std::min(c.streams, 16) : kDefaultLanes);
     if ((e = cudaEventCreateWithFlags(&h->ev_device, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreate(&h->ev_dk0)) != cudaSuccess || (e = cudaEventCreate(&h->ev_dk1)) != cudaSuccess) {
         sbfs_destroy(h);
@@ -733,11 +733,11 @@ int32_t sbfs_describe_plan(sbfs_handle *h, char *buf, int32_t len)
     }
     const Plan &P = h->plan;
     std::string js = "{\"small_kernel\":\"";
-    js += h->cfg.small_kernel == 1 ? "lane" : "pool";
+    js += h->cfg.small_kernel == 2 ? "pool" : "lane";
     js += "\",\"classes\":[";
     char tmp[256];
     for (int c = 0; c < 3; ++c) {
-        const bool lane = c < 2 && h->cfg.small_kernel == 1;
+        const bool lane = c < 2 && h->cfg.small_kernel != 2;
         if (lane) {
             const LaneShape &l = P.lane[c];
             std::snprintf(tmp, sizeof tmp,

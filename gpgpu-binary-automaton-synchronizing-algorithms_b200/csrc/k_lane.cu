@@ -1,7 +1,7 @@
 // k_lane.cu -- power-set BFS with one automaton per lane (n <= 12).
 //
 // Each lane runs the sequential BFS of GPGPU/CPU/SlimCPU4bits.cs:214-306 on its
-// own automaton: pop a subset, look up both images in its nibble table
+// own automaton: pop subsets, look up both images in its nibble table
 // (entry = a-image << 16 | b-image, SlimCPU4bits.cs:122-206), test-and-set them
 // in its visited bitmap, append the new ones, advance the level when the
 // current level is used up (SlimCPUUntweaked.cs:126-130,160-164), stop at the
@@ -11,13 +11,20 @@
 // Shared memory is lane-interleaved: element e of lane l's bitmap, table and
 // queue lives at [e][l], so every lane-private access of a warp touches 32
 // different banks.  The queue is a ring of R entries holding only the live
-// frontier (current level remainder + next level); each entry carries the
-// letters of the word that reaches it (bit NMAX + d = letter d, 1 = b), so a
-// word needs no parent pointers or retained history.
+// frontier (current level remainder + next level); with words requested each
+// entry carries the letters of the word that reaches it (bit NMAX + d =
+// letter d, 1 = b), so a word needs no parent pointers or retained history.
 //
-// Two rare cases leave this kernel: a frontier wider than R, and a word longer
-// than 32 - NMAX letters.  Such an automaton is abandoned and appended to an
-// escalation list that the warp-pooled kernel (k_pool.cu) solves afterwards.
+// Each iteration a lane takes up to two subsets of its current level.  Their
+// four images are tested in queue order (first subset's a, b, then the
+// second's), exactly as the sequential loop would; the four bitmap words are
+// loaded up front and a word touched twice is forwarded in registers, so the
+// test-and-sets do not wait on one another's shared-memory round trips.
+//
+// Two rare cases leave this kernel: a frontier wider than R, and (with words)
+// a word longer than 32 - NMAX letters.  Such an automaton is abandoned and
+// appended to an escalation list that the warp-pooled kernel (k_pool.cu)
+// solves afterwards.
 //
 // Lanes that finish wait until `refill_k` lanes of the warp are idle; then the
 // warp writes their results and loads new automata for all of them in one
@@ -45,6 +52,15 @@ struct LaneGeom {
 };
 
 template <int NMAX>
+__device__ __forceinline__ uint32_t lane_image(const uint32_t *tb, uint32_t x)
+{
+    uint32_t t = tb[(x & 15u) * 32];
+    if (LaneGeom<NMAX>::kChunks > 1) t |= tb[(16 + ((x >> 4) & 15u)) * 32];
+    if (LaneGeom<NMAX>::kChunks > 2) t |= tb[(32 + ((x >> 8) & 15u)) * 32];
+    return t;
+}
+
+template <int NMAX, bool WORDS>
 __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, int32_t *escal_list,
                                               unsigned long long *escal_count, unsigned long long *ticket)
 {
@@ -63,7 +79,6 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
     int64_t count;
     const int32_t *order;
     resolve_work(b, count, order);
-    const bool words = b.out_words != nullptr;
 
     int state = kIdle;
     int64_t k = -1;
@@ -77,11 +92,11 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
     while (true) {
         // ---- phase: finish waiting lanes, load new automata -----------------
         const unsigned not_active = __ballot_sync(kFull, state != kActive);
-        const unsigned waiting = __ballot_sync(kFull, state == kDone || state == kEscalate);
-        if (not_active == kFull || (__popc(not_active) >= refill_k && (more || waiting))) {
+        if (not_active == kFull ||
+            (__popc(not_active) >= refill_k && (more || __any_sync(kFull, state == kDone || state == kEscalate)))) {
             if (state == kDone) {
                 record_result(b, k, n, res_len);
-                if (b.out_words) {
+                if (WORDS) {
                     uint64_t *w = b.out_words + (size_t)k * (size_t)b.word_stride;
                     w[0] = res_len > 0 ? (uint64_t)res_word : 0ull;
                     for (int c = 1; c < b.word_stride; ++c) w[c] = 0ull;
@@ -111,11 +126,9 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
                         state = kActive;
                     }
                 }
-                bool bad = false;
                 // every lane that just received an automaton sets it up
-                const bool fresh = (state == kActive) && (idle & (1u << lane));
-                if (fresh) {
-                    if (n < 1 || n > NMAX || n > b.lstride) bad = true;
+                if (state == kActive && (idle & (1u << lane))) {
+                    bool bad = (n < 1 || n > NMAX || n > b.lstride);
                     const uint8_t *rec = b.maps + (size_t)k * 2u * (size_t)b.lstride;
                     uint32_t aw[G::kChunks] = {}, bw[G::kChunks] = {};
                     if (!bad) {
@@ -130,8 +143,6 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
                         } else {
 #pragma unroll
                             for (int c = 0; c < G::kChunks; ++c) {
-                                aw[c] = 0u;
-                                bw[c] = 0u;
 #pragma unroll
                                 for (int j = 0; j < 4; ++j) {
                                     if (4 * c + j < n) {
@@ -149,12 +160,9 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
                         for (int j = 0; j < 4; ++j) {
                             const int st = 4 * c + j;
                             const uint32_t av = (aw[c] >> (8 * j)) & 0xFFu, bv = (bw[c] >> (8 * j)) & 0xFFu;
-                            if (bad || st >= n) {
-                                s[j] = 0u;
-                            } else {
-                                if (av >= (uint32_t)n || bv >= (uint32_t)n) bad = true;
-                                s[j] = (1u << ((av & 15u) + 16)) | (1u << (bv & 15u));
-                            }
+                            const bool in = !bad && st < n;
+                            if (in && (av >= (uint32_t)n || bv >= (uint32_t)n)) bad = true;
+                            s[j] = in ? ((1u << ((av & 15u) + 16)) | (1u << (bv & 15u))) : 0u;
                         }
                         // table[c*16 + v] = OR of s[j] over the set bits j of v
                         uint32_t t[16];
@@ -169,7 +177,7 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
                         atomicOr(b.error, kErrInvalid);
                         state = kIdle;
                     } else {
-#pragma unroll 8
+#pragma unroll 16
                         for (int w = 0; w < BW; ++w) bm[w * 32] = 0u;
                         const uint32_t full = (1u << n) - 1u;
                         bm[(full >> 5) * 32] = 1u << (full & 31u);
@@ -187,40 +195,52 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
             }
         }
 
-        // ---- one expansion per active lane ----------------------------------
+        // ---- up to two expansions per active lane ----------------------------
         if (state == kActive) {
-            const uint32_t e = rq[(head & rmask) * 32];
-            ++head;
-            ++expanded;
-            const uint32_t x = e & G::kMask;
-            const uint32_t wbits = e >> NMAX;
-            uint32_t t = tb[(x & 15u) * 32];
-            if (G::kChunks > 1) t |= tb[(16 + ((x >> 4) & 15u)) * 32];
-            if (G::kChunks > 2) t |= tb[(32 + ((x >> 8) & 15u)) * 32];
-            const uint32_t ya = t >> 16, yb = t & 0xFFFFu;
+            const bool two = head + 1u < lvl_end;
+            const uint32_t e0 = rq[(head & rmask) * 32];
+            const uint32_t e1 = two ? rq[((head + 1u) & rmask) * 32] : 0u;
+            head += two ? 2u : 1u;
+            expanded += two ? 2u : 1u;
+            const uint32_t t0 = lane_image<NMAX>(tb, e0 & G::kMask);
+            const uint32_t t1 = lane_image<NMAX>(tb, e1 & G::kMask);
+            const uint32_t y[4] = {t0 >> 16, t0 & 0xFFFFu, t1 >> 16, t1 & 0xFFFFu};
+            uint32_t wd[4], mk[4], wv[4];
 #pragma unroll
-            for (int letter = 0; letter < 2; ++letter) {
-                if (state != kActive) break;
-                const uint32_t y = letter ? yb : ya;
-                uint32_t *wp = bm + (y >> 5) * 32;
-                const uint32_t m = 1u << (y & 31u);
-                const uint32_t wv = *wp;
-                if (!(wv & m)) {
-                    if (is_singleton(y)) {
-                        state = kDone;
-                        res_len = (int32_t)level + 1;
-                        res_word = words ? (wbits | ((uint32_t)letter << level)) : 0u;
-                    } else if (tail - head >= (uint32_t)ring || (words && level >= (uint32_t)G::kWordMax)) {
+            for (int c = 0; c < 4; ++c) {
+                wd[c] = y[c] >> 5;
+                mk[c] = 1u << (y[c] & 31u);
+                wv[c] = (c < 2 || two) ? bm[wd[c] * 32] : kFull;
+            }
+            bool stop = false;
+            bool pushed[4] = {false, false, false, false};
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                // bits set earlier in this iteration in the same bitmap word
+#pragma unroll
+                for (int p = 0; p < c; ++p)
+                    if (pushed[p] && wd[p] == wd[c]) wv[c] |= mk[p];
+                const bool fresh = !stop && !(wv[c] & mk[c]);
+                const uint32_t wbits = WORDS ? ((c < 2 ? e0 : e1) >> NMAX) : 0u;
+                const uint32_t letter = (uint32_t)(c & 1);
+                if (fresh && is_singleton(y[c])) {
+                    stop = true;
+                    state = kDone;
+                    res_len = (int32_t)level + 1;
+                    res_word = WORDS ? (wbits | (letter << level)) : 0u;
+                } else if (fresh) {
+                    if (tail - head >= (uint32_t)ring || (WORDS && level >= (uint32_t)G::kWordMax)) {
+                        stop = true;
                         state = kEscalate;
                     } else {
-                        *wp = wv | m;
-                        rq[(tail & rmask) * 32] =
-                            words ? (y | ((wbits | ((uint32_t)letter << level)) << NMAX)) : y;
+                        pushed[c] = true;
+                        bm[wd[c] * 32] = wv[c] | mk[c];
+                        rq[(tail & rmask) * 32] = WORDS ? (y[c] | ((wbits | (letter << level)) << NMAX)) : y[c];
                         ++tail;
                     }
                 }
             }
-            if (state == kActive && head == lvl_end) {
+            if (!stop && head == lvl_end) {
                 if (tail == lvl_end) {
                     state = kDone;
                     res_len = kLenNonSync;
@@ -242,8 +262,16 @@ size_t smem_for(int warps, int ring)
     return (size_t)warps * (G::kBitmapWords + G::kTable + ring) * 32 * sizeof(uint32_t);
 }
 
-template <int NMAX>
-const void *kptr() { return (const void *)k_lane<NMAX>; }
+template <int NMAX, bool WORDS>
+cudaError_t launch_t(int warps, int ring, int refill_k, int ctas, const Batch &b, int32_t *escal_list,
+                     unsigned long long *escal_count, unsigned long long *ticket, cudaStream_t st)
+{
+    const size_t smem = smem_for<NMAX>(warps, ring);
+    cudaError_t e = cudaFuncSetAttribute(k_lane<NMAX, WORDS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_lane<NMAX, WORDS><<<ctas, warps * 32, smem, st>>>(b, ring, refill_k, escal_list, escal_count, ticket);
+    return cudaGetLastError();
+}
 
 }  // namespace
 
@@ -254,7 +282,7 @@ size_t lane_smem_bytes(int nmax, int warps, int ring)
 
 int lane_max_ctas_per_sm(int nmax, int warps, int ring)
 {
-    const void *k = nmax <= 8 ? kptr<8>() : kptr<12>();
+    const void *k = nmax <= 8 ? (const void *)k_lane<8, true> : (const void *)k_lane<12, true>;
     const size_t smem = lane_smem_bytes(nmax, warps, ring);
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         cudaGetLastError();
@@ -274,19 +302,14 @@ cudaError_t launch_lane(int nmax, int warps, int ring, int refill_k, int ctas, c
 {
     if ((ring & (ring - 1)) || ring < 8 || warps < 1 || warps > 8 || ctas < 1 || refill_k < 1 || refill_k > 32)
         return cudaErrorInvalidValue;
-    const size_t smem = lane_smem_bytes(nmax, warps, ring);
-    if (nmax <= 8) {
-        cudaError_t e = cudaFuncSetAttribute(k_lane<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        k_lane<8><<<ctas, warps * 32, smem, st>>>(b, ring, refill_k, escal_list, escal_count, ticket);
-    } else if (nmax <= 12) {
-        cudaError_t e = cudaFuncSetAttribute(k_lane<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        k_lane<12><<<ctas, warps * 32, smem, st>>>(b, ring, refill_k, escal_list, escal_count, ticket);
-    } else {
-        return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
+    const bool words = b.out_words != nullptr;
+    if (nmax <= 8)
+        return words ? launch_t<8, true>(warps, ring, refill_k, ctas, b, escal_list, escal_count, ticket, st)
+                     : launch_t<8, false>(warps, ring, refill_k, ctas, b, escal_list, escal_count, ticket, st);
+    if (nmax <= 12)
+        return words ? launch_t<12, true>(warps, ring, refill_k, ctas, b, escal_list, escal_count, ticket, st)
+                     : launch_t<12, false>(warps, ring, refill_k, ctas, b, escal_list, escal_count, ticket, st);
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace sbfs

@@ -50,6 +50,7 @@ class Config(ctypes.Structure):
         ("lane_ring", ctypes.c_int32),
         ("lane_refill", ctypes.c_int32),
         ("lane_warps", ctypes.c_int32),
+        ("streams", ctypes.c_int32),
         ("tune_cache", ctypes.c_char_p),
     ]
 

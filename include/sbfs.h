@@ -82,10 +82,11 @@ typedef struct sbfs_config {
     int32_t warps_per_cta;     /* small-n kernel: warps per CTA; 0 = auto               */
     int32_t queue_smem;        /* small-n kernel: on-chip queue entries per automaton; 0 = auto */
     int32_t chunk;             /* host<->device pipeline chunk (automata); 0 = auto     */
-    int32_t small_kernel;      /* n <= 12: 0 = auto, 1 = one automaton per lane, 2 = warp-pooled */
+    int32_t small_kernel;      /* n <= 12: 0 = auto (per lane), 1 = one automaton per lane, 2 = warp-pooled */
     int32_t lane_ring;         /* per-lane kernel: on-chip frontier entries (power of 2); 0 = auto */
     int32_t lane_refill;       /* per-lane kernel: idle lanes that trigger a refill; 0 = auto */
     int32_t lane_warps;        /* per-lane kernel: warps per CTA; 0 = auto              */
+    int32_t streams;           /* streams the host path rotates chunks over; 0 = 4      */
     const char *tune_cache;    /* autotuner cache file, or NULL for in-memory only      */
 } sbfs_config;
 
