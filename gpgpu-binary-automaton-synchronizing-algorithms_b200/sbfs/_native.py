@@ -18,7 +18,7 @@ EXPORTS = [
     "sbfs_abi_version", "sbfs_config_default", "sbfs_create", "sbfs_destroy", "sbfs_last_error",
     "sbfs_status_string", "sbfs_best_parallelism", "sbfs_solve_batch", "sbfs_verify_batch",
     "sbfs_solve_plain", "sbfs_solve_batch_device", "sbfs_device_wait", "sbfs_host_alloc",
-    "sbfs_host_free", "sbfs_word_stride", "sbfs_describe_plan",
+    "sbfs_host_free", "sbfs_word_stride", "sbfs_describe_plan", "sbfs_solve_small_noalloc",
 ]
 
 STATUS = {0: "SBFS_OK", 1: "SBFS_EINVAL", 2: "SBFS_ENOMEM", 3: "SBFS_ETIMEOUT", 4: "SBFS_ECUDA",
@@ -115,6 +115,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.sbfs_device_wait.restype = ctypes.c_int
     L.sbfs_host_alloc.argtypes = [ctypes.c_size_t, ctypes.POINTER(P)]
     L.sbfs_host_alloc.restype = ctypes.c_int
+    L.sbfs_solve_small_noalloc.argtypes = [P, i32, i32, i64, P, P, i32, P, P]
+    L.sbfs_solve_small_noalloc.restype = ctypes.c_int
     L.sbfs_describe_plan.argtypes = [P, ctypes.c_char_p, i32]
     L.sbfs_describe_plan.restype = i32
     L.sbfs_host_free.argtypes = [P]

@@ -163,6 +163,27 @@ SBFS_API sbfs_status sbfs_device_wait(sbfs_handle *h, sbfs_stats *stats);
 SBFS_API sbfs_status sbfs_host_alloc(size_t bytes, void **out);
 SBFS_API sbfs_status sbfs_host_free(void *p);
 
+/*
+ * Allocation-free solve for callers that must not allocate device memory: a
+ * plugin inside a process whose framework already owns the device memory
+ * budget (a new cudaMalloc would fail or evict its cache), or a tight serving
+ * loop where cudaMalloc/cudaFree would synchronise the device.  This entry
+ * point has no counterpart in the reference.  It takes no handle: it solves
+ * count automata with 1 <= n <= 12 states (d_maps, d_len, d_words and
+ * *d_first_violation are caller-owned device memory) on the current device,
+ * enqueued on `stream` (a cudaStream_t; NULL = the default stream), and keeps
+ * all of its working memory in one fixed 16 MiB array inside the library.
+ * n > 12 returns SBFS_EINVAL.  Every call shares that array, so calls that
+ * overlap on the GPU race; serialise them.  The first call on a device looks
+ * the array up (cudaGetSymbolAddress); make it before any stream capture.
+ * A malformed record gets length -2 in d_len.  Words and lengths follow the
+ * conventions above; it is slower than sbfs_solve_batch_device.
+ */
+SBFS_API sbfs_status sbfs_solve_small_noalloc(const uint8_t *d_maps, int32_t lstride, int32_t n,
+                                              int64_t count, int32_t *d_len, uint64_t *d_words,
+                                              int32_t word_stride, int64_t *d_first_violation,
+                                              void *stream);
+
 /* JSON description of the kernel plan the handle uses (kernel and shape per
  * size class), written to buf (NUL-terminated, truncated to len).  Returns
  * the full length needed. */
