@@ -28,10 +28,6 @@ size_t cta_queue_entries(int nb_max, int ctas);
 int cta_max_ctas_per_sm(int nb_max, int threads);
 cudaError_t launch_cta(int nb_max, int threads, int ctas, const Batch &b, uint64_t *queues,
                        unsigned long long *ticket, cudaStream_t st);
-size_t hbm_ctl_bytes();
-int hbm_max_ctas_per_sm(int threads);
-cudaError_t launch_hbm(int threads, int ctas, const Batch &b, uint32_t *bitmap, uint64_t *queue,
-                       void *ctl, unsigned long long *ticket, cudaStream_t st);
 cudaError_t plan_autotune(sbfs_handle *h, Plan &plan);
 
 cudaError_t DevBuf::reserve(size_t want)
@@ -148,6 +144,83 @@ int class_present_mask(const Job &j)
     return m;
 }
 
+size_t level_arena_bytes(sbfs_handle *h, int max_n)
+{
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        free_b = (size_t)8 << 30;
+    }
+    size_t want = free_b / 2;
+    const size_t cap = (size_t)64 << 30;
+    if (want > cap) want = cap;
+    const size_t one = LevelEngine::footprint(max_n);
+    if (want < one) want = one;   // at least one automaton of the largest size
+    (void)h;
+    return want;
+}
+
+// Automata with 21 <= n <= 28 run on the device-resident level slots: admit as
+// many as the arena holds, advance them a few levels per launch batch, collect
+// the finished ones, admit more.  Results land in the job's device outputs.
+sbfs_status run_level_class(sbfs_handle *h, Lane &L, const Job &j, const Batch &bc, int *launches)
+{
+    std::vector<std::pair<int64_t, int>> items;
+    if (!j.ns) {
+        items.reserve((size_t)j.count);
+        for (int64_t i = 0; i < j.count; ++i) items.push_back({i, j.n_uniform});
+    } else {
+        // class-4 members come from the device bucketing: read the range, the order slice and sizes
+        unsigned long long range[2] = {0, 0};
+        CK(cudaMemcpyAsync(range, bc.range_dev, sizeof(range), cudaMemcpyDeviceToHost, L.stream),
+           "reading class range");
+        CK(cudaStreamSynchronize(L.stream), "waiting for bucketing");
+        if (range[1] == 0) return SBFS_OK;
+        std::vector<int32_t> idx((size_t)range[1]);
+        std::vector<uint8_t> ns((size_t)j.count);
+        CK(cudaMemcpy(idx.data(), bc.order + range[0], idx.size() * sizeof(int32_t), cudaMemcpyDeviceToHost),
+           "reading class members");
+        CK(cudaMemcpy(ns.data(), j.ns, ns.size(), cudaMemcpyDeviceToHost), "reading sizes");
+        for (int32_t i : idx) items.push_back({i, ns[(size_t)i]});
+    }
+    if (items.empty()) return SBFS_OK;
+    int max_n = 0;
+    for (auto &it : items) max_n = std::max(max_n, it.second);
+    max_n = std::min(std::max(max_n, 1), SBFS_MAX_N);
+    if (!L.level_ready) {
+        CK(L.level.init(h->sm_count, level_arena_bytes(h, max_n), L.stream), "setting up level slots");
+        L.level_ready = true;
+    } else if (L.level.arena_capacity() < LevelEngine::footprint(max_n)) {
+        L.level.destroy();
+        CK(L.level.init(h->sm_count, level_arena_bytes(h, max_n), L.stream), "setting up level slots");
+    }
+    LevelEngine &E = L.level;
+    size_t next = 0;
+    int levels = 4;
+    std::vector<LevelEngine::Finished> done;
+    const size_t rec = 2 * (size_t)j.lstride;
+    while (next < items.size() || E.in_flight() > 0) {
+        while (next < items.size()) {
+            const int n = items[next].second;
+            if (n < 21 || n > SBFS_MAX_N) return fail(h, SBFS_EINVAL, "n out of range for the level class");
+            if (E.admit(j.maps + (size_t)items[next].first * rec, j.lstride, n, items[next].first, nullptr,
+                        nullptr) < 0)
+                break;
+            ++next;
+        }
+        if (E.in_flight() == 0) return fail(h, SBFS_ENOMEM, "level-slot arena cannot hold one automaton");
+        CK(E.launch(levels, bc), "launching level kernels");
+        *launches += levels;
+        done.clear();
+        CK(E.collect(done), "collecting level slots");
+        for (auto &f : done)
+            if (f.state == kSlotFail) return fail(h, SBFS_ECUDA, "level slot queue overflow");
+        // long-running automata: fewer host round trips
+        levels = done.empty() ? std::min(levels * 2, 256) : 4;
+    }
+    return SBFS_OK;
+}
+
 // Reserve the lane's work buffers for a job and enqueue its kernels on the lane's
 // stream.  Counters must already be reset.
 sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches, bool plain = false,
@@ -207,17 +280,9 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
             CK(launch_cta(nb, P.cta.threads, ctas, bc, L.cta_queue.as<uint64_t>(), ticket, st),
                "launching n<=20 kernel");
         } else {
-            const int nb = std::min(28, std::max(j.ns ? j.max_n : j.n_uniform, 21));
-            const size_t bitmap_bytes = ((size_t)1 << nb) / 8;
-            CK(L.hbm_bitmap.reserve(bitmap_bytes + hbm_ctl_bytes()), "allocating HBM bitmap");
-            CK(L.hbm_queue.reserve(((size_t)1 << nb) * sizeof(uint64_t)), "allocating HBM queue");
-            const int per_sm = hbm_max_ctas_per_sm(P.hbm.threads);
-            if (per_sm < 1) return fail(h, SBFS_ECUDA, "HBM kernel does not fit on an SM");
-            const int ctas = std::min(P.hbm.ctas, per_sm * h->sm_count);
-            void *ctl = L.hbm_bitmap.as<char>() + bitmap_bytes;
-            CK(launch_hbm(P.hbm.threads, ctas, bc, L.hbm_bitmap.as<uint32_t>(), L.hbm_queue.as<uint64_t>(),
-                          ctl, ticket, st),
-               "launching n<=28 kernel");
+            sbfs_status ls = run_level_class(h, L, j, bc, launches);
+            if (ls) return ls;
+            continue;
         }
         *launches += 1;
     }
@@ -504,6 +569,23 @@ sbfs_status solve_host(sbfs_handle *h, const uint8_t *maps, int32_t lstride, con
 
 }  // namespace
 
+namespace sbfs {
+
+// Enqueue one solve of device-resident records on lane L's stream (counters
+// reset, size-class bucketing, class kernels).  Shared with the serving loop.
+sbfs_status engine_enqueue(sbfs_handle *h, Lane &L, const uint8_t *d_maps, int32_t lstride, const uint8_t *d_ns,
+                           int32_t n_uniform, int32_t max_n, int64_t count, int32_t *d_len, uint64_t *d_words,
+                           int32_t word_stride, int *launches)
+{
+    sbfs_status s = ensure_plan(h);
+    if (s) return s;
+    if ((s = reset_counters(h, L))) return s;
+    Job j{d_maps, lstride, d_ns, n_uniform, max_n, count, d_len, d_words, d_words ? word_stride : 0};
+    return enqueue_kernels(h, L, j, launches);
+}
+
+}  // namespace sbfs
+
 extern "C" {
 
 int32_t sbfs_abi_version(void) { return SBFS_ABI_VERSION; }
@@ -590,6 +672,7 @@ sbfs_status sbfs_destroy(sbfs_handle *h)
         if (L.ev_k0) cudaEventDestroy(L.ev_k0);
         if (L.ev_k1) cudaEventDestroy(L.ev_k1);
         if (L.ev_done) cudaEventDestroy(L.ev_done);
+        if (L.level_ready) L.level.destroy();
         if (L.stream) cudaStreamDestroy(L.stream);
     }
     if (h->ev_device) cudaEventDestroy(h->ev_device);
@@ -755,8 +838,8 @@ int32_t sbfs_describe_plan(sbfs_handle *h, char *buf, int32_t len)
     }
     std::snprintf(tmp, sizeof tmp,
                   "{\"class\":3,\"max_n\":20,\"kernel\":\"k_cta\",\"threads\":%d,\"ctas\":%d},"
-                  "{\"class\":4,\"max_n\":28,\"kernel\":\"k_hbm\",\"threads\":%d,\"ctas\":%d}]}",
-                  P.cta.threads, P.cta.ctas, P.hbm.threads, P.hbm.ctas);
+                  "{\"class\":4,\"max_n\":28,\"kernel\":\"k_level\",\"threads\":512,\"slots\":%d}]}",
+                  P.cta.threads, P.cta.ctas, kMaxLevelSlots);
     js += tmp;
     if (buf && len > 0) {
         std::strncpy(buf, js.c_str(), (size_t)len - 1);

@@ -1,0 +1,278 @@
+// k_level.cu -- level-synchronous power-set BFS of many large automata at
+// once, with every automaton's visited bitmap and frontier in HBM.
+//
+// State lives in device memory between launches ("slots"): each admitted
+// automaton owns a 2^n-bit bitmap, a queue of 64-bit entries
+// (subset | parent index << 28 | letter-is-b << 63, retained for the word as
+// in GPGPU/CPU/CPU.cs:203-205,262-269) and byte tables of its images.  One
+// launch of k_level advances every running slot by exactly one BFS level:
+// all CTAs stride over the concatenation of the slots' current levels, test-
+// and-set images in the bitmaps with global atomics, and append new subsets
+// through a per-CTA staging buffer (one global atomic per slot per CTA round,
+// coalesced writes).  The last CTA to finish (threadfence + ticket, no spin)
+// then moves every slot to its next level, finishes the ones that found a
+// singleton or ran dry, turns freshly admitted slots into running ones, and
+// recomputes the prefix sums the next launch uses.  Level semantics are those
+// of GPGPU/CPU/SlimCPUUntweaked.cs:119-184.
+//
+// Because state persists, the host (batch path or the serving loop) can admit
+// new automata into free slots between launches and launch levels back to
+// back (or from a CUDA graph) without waiting for the slowest automaton.
+#include "level.cuh"
+
+namespace sbfs {
+namespace {
+
+constexpr int kThreads = 512;
+constexpr int kStage = 2 * kThreads;   // staged pushes per CTA round
+
+__device__ __forceinline__ int find_slot(const unsigned long long *prefix, int nslots, unsigned long long item)
+{
+    // largest s with prefix[s] <= item (prefix[0] = 0, nondecreasing)
+    int lo = 0, hi = nslots;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (prefix[mid] <= item)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kThreads) k_level(LevelSlot *slots, uint64_t *tables, LevelCtl *ctl,
+                                                    Batch out)
+{
+    __shared__ unsigned long long s_prefix[kMaxLevelSlots + 1];
+    __shared__ uint64_t s_stage[kStage];
+    __shared__ unsigned short s_stage_slot[kStage];
+    __shared__ unsigned int s_count;
+    __shared__ unsigned int s_slot_count[kMaxLevelSlots];
+    __shared__ unsigned long long s_slot_base[kMaxLevelSlots];
+    __shared__ bool s_last;
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int nslots = ctl->nslots;
+    const unsigned long long total = ctl->total;
+    for (int i = tid; i <= nslots; i += blockDim.x) s_prefix[i] = ctl->prefix[i];
+
+    // ---- set-up of freshly admitted slots: clear bitmaps, build tables ------
+    const size_t gtid = (size_t)blockIdx.x * blockDim.x + tid;
+    const size_t gthreads = (size_t)gridDim.x * blockDim.x;
+    for (int q = 0; q < ctl->n_init; ++q) {
+        const int s = ctl->init_list[q];
+        LevelSlot &sl = slots[s];
+        const size_t words4 = sl.n >= 7 ? ((size_t)1 << sl.n) / 128 : 1;
+        uint4 *bm4 = reinterpret_cast<uint4 *>(sl.bitmap);
+        for (size_t w = gtid; w < words4; w += gthreads) bm4[w] = make_uint4(0u, 0u, 0u, 0u);
+        uint64_t *tb = tables + (size_t)s * kLevelTable;
+        for (size_t e = gtid; e < kLevelTable; e += gthreads) {
+            const int c = (int)(e >> 8), v = (int)(e & 255);
+            uint32_t ta = 0, tbv = 0;
+            for (int j = 0; j < 8; ++j) {
+                const int st = 8 * c + j;
+                if (((v >> j) & 1) && st < sl.n) {
+                    const uint32_t av = sl.rec ? sl.rec[st] : sl.a[st];
+                    const uint32_t bv = sl.rec ? sl.rec[sl.lstride + st] : sl.b[st];
+                    ta |= 1u << (av & 31u);
+                    tbv |= 1u << (bv & 31u);
+                }
+            }
+            tb[e] = ((uint64_t)ta << 32) | tbv;
+        }
+    }
+    if (tid < kMaxLevelSlots) s_slot_count[tid] = 0;
+    __syncthreads();
+
+    // ---- one level of every running slot ------------------------------------
+    unsigned long long expanded = 0;
+    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < total;
+         base += gthreads) {
+        if (tid == 0) s_count = 0;
+        __syncthreads();
+        const unsigned long long item = base + tid;
+        if (item < total) {
+            const int s = find_slot(s_prefix, nslots, item);
+            LevelSlot &sl = slots[s];
+            const unsigned long long idx = sl.lvl_start + (item - s_prefix[s]);
+            const uint32_t x = (uint32_t)(__ldcg(sl.queue + idx) & kLevelSubsetMask);
+            const uint64_t *tb = tables + (size_t)s * kLevelTable;
+            uint64_t t = __ldg(tb + (x & 255u));
+            t |= __ldg(tb + 256 + ((x >> 8) & 255u));
+            t |= __ldg(tb + 512 + ((x >> 16) & 255u));
+            t |= __ldg(tb + 768 + ((x >> 24) & 255u));
+            ++expanded;
+#pragma unroll
+            for (int letter = 0; letter < 2; ++letter) {
+                const uint32_t y = letter ? (uint32_t)t : (uint32_t)(t >> 32);
+                const uint32_t m = 1u << (y & 31u);
+                if (!(atomicOr(sl.bitmap + (y >> 5), m) & m)) {
+                    if (is_singleton(y)) {
+                        atomicMin(&sl.found, (idx << 1) | (unsigned long long)letter);
+                    } else {
+                        const unsigned int pos = atomicAdd(&s_count, 1u);
+                        s_stage[pos] = (uint64_t)y | (idx << 28) | ((uint64_t)letter << 63);
+                        s_stage_slot[pos] = (unsigned short)s;
+                        atomicAdd(&s_slot_count[s], 1u);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // reserve space per slot: one global atomic per slot with pushes this round
+        for (int s = tid; s < nslots; s += blockDim.x) {
+            const unsigned int c = s_slot_count[s];
+            if (c) {
+                s_slot_base[s] = atomicAdd(&slots[s].tail, (unsigned long long)c);
+                s_slot_count[s] = 0;
+            }
+        }
+        __syncthreads();
+        const unsigned int cnt = s_count;
+        for (unsigned int p = tid; p < cnt; p += blockDim.x) {
+            const int s = s_stage_slot[p];
+            const unsigned long long pos = atomicAdd(&s_slot_base[s], 1ull);
+            LevelSlot &sl = slots[s];
+            if (pos < sl.cap)
+                __stcg(sl.queue + pos, s_stage[p]);
+            else
+                atomicOr(&sl.overflow, 1);
+        }
+        __syncthreads();
+    }
+    for (int o = 16; o; o >>= 1) expanded += __shfl_down_sync(kFull, expanded, o);
+    if (lane == 0 && expanded) atomicAdd(&ctl->expanded, expanded);
+
+    // ---- the last CTA moves every slot to its next level ---------------------
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) s_last = atomicAdd(&ctl->done_ctas, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    for (int s = tid; s < nslots; s += blockDim.x) {
+        LevelSlot &sl = slots[s];
+        const int st = *(volatile int *)&sl.state;
+        if (st == kSlotInit) {
+            bool bad = sl.n < 1 || sl.n > 28;
+            for (int j = 0; !bad && j < sl.n; ++j) {
+                const uint32_t av = sl.rec ? sl.rec[j] : sl.a[j];
+                const uint32_t bv = sl.rec ? sl.rec[sl.lstride + j] : sl.b[j];
+                if (av >= (uint32_t)sl.n || bv >= (uint32_t)sl.n) bad = true;
+            }
+            if (bad) {
+                sl.result_len = kLenInvalid;
+                for (int c = 0; c < kLevelWordU64; ++c) sl.word[c] = 0ull;
+                if (out.out_len && sl.tag >= 0) out.out_len[sl.tag] = kLenInvalid;
+                if (out.error) atomicOr(out.error, kErrInvalid);
+                sl.state = kSlotDone;
+                atomicAdd(&ctl->finished, 1u);
+                continue;
+            }
+            const uint32_t full = sl.n >= 32 ? 0xFFFFFFFFu : (1u << sl.n) - 1u;
+            sl.queue[0] = full;
+            sl.bitmap[full >> 5] = 1u << (full & 31u);
+            sl.lvl_start = 0;
+            sl.lvl_end = 1;
+            sl.tail = 1;
+            sl.level = 0;
+            sl.found = ~0ull;
+            sl.overflow = 0;
+            sl.state = kSlotRun;
+        } else if (st == kSlotRun) {
+            const unsigned long long f = *(volatile unsigned long long *)&sl.found;
+            const unsigned long long tail = *(volatile unsigned long long *)&sl.tail;
+            int32_t len = 0;
+            int next = kSlotRun;
+            if (f != ~0ull) {
+                len = (int32_t)sl.level + 1;
+                next = kSlotDone;
+            } else if (sl.overflow || tail > sl.cap) {
+                len = kLenNonSync;
+                next = kSlotFail;
+            } else if (tail == sl.lvl_end) {
+                len = kLenNonSync;
+                next = kSlotDone;
+            }
+            if (next == kSlotRun) {
+                sl.lvl_start = sl.lvl_end;
+                sl.lvl_end = tail;
+                ++sl.level;
+            } else {
+                sl.result_len = len;
+                for (int c = 0; c < kLevelWordU64; ++c) sl.word[c] = 0ull;
+                if (next == kSlotDone && len > 0 && len <= 64 * kLevelWordU64) {
+                    int d = len - 1;
+                    sl.word[d >> 6] |= (uint64_t)(f & 1ull) << (d & 63);
+                    uint64_t e = __ldcg(sl.queue + (f >> 1));
+                    for (d = len - 2; d >= 0; --d) {
+                        sl.word[d >> 6] |= (uint64_t)(e >> 63) << (d & 63);
+                        e = __ldcg(sl.queue + ((e >> 28) & 0x7FFFFFFFFull));
+                    }
+                }
+                if (out.out_len && sl.tag >= 0 && next == kSlotDone) {
+                    record_result(out, sl.tag, sl.n, len);
+                    if (out.out_words) {
+                        uint64_t *w = out.out_words + (size_t)sl.tag * (size_t)out.word_stride;
+                        for (int c = 0; c < out.word_stride; ++c) w[c] = c < kLevelWordU64 ? sl.word[c] : 0ull;
+                    }
+                }
+                sl.state = next;
+                atomicAdd(&ctl->finished, 1u);
+            }
+        }
+    }
+    // prefix sums of the new levels (block-wide scan over the slots)
+    __shared__ unsigned long long s_width[kMaxLevelSlots];
+    __shared__ unsigned long long s_warp[kThreads / 32];
+    __syncthreads();
+    unsigned long long w = 0;
+    if (tid < nslots && slots[tid].state == kSlotRun) w = slots[tid].lvl_end - slots[tid].lvl_start;
+    if (tid < kMaxLevelSlots) s_width[tid] = w;
+    unsigned long long incl = w;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const unsigned long long y = __shfl_up_sync(kFull, incl, d);
+        if (lane >= d) incl += y;
+    }
+    if (lane == 31) s_warp[tid >> 5] = incl;
+    __syncthreads();
+    unsigned long long before = 0;
+    for (int q = 0; q < (tid >> 5); ++q) before += s_warp[q];
+    const unsigned long long excl = before + incl - w;
+    if (tid <= nslots) ctl->prefix[tid] = excl;   // prefix[nslots] = total (w = 0 there)
+    const int running = __syncthreads_count(w > 0);
+    if (tid == 0) {
+        unsigned long long total_new = 0;
+        for (int q = 0; q < kThreads / 32; ++q) total_new += s_warp[q];
+        ctl->total = total_new;
+        ctl->running = running;
+        ctl->n_init = 0;
+        ctl->launches += 1;
+        ctl->done_ctas = 0;
+        __threadfence();
+    }
+}
+
+}  // namespace
+
+int level_max_ctas_per_sm()
+{
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_level, kThreads, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return blocks;
+}
+
+cudaError_t launch_level(int ctas, LevelSlot *slots, uint64_t *tables, LevelCtl *ctl, const Batch &out,
+                         cudaStream_t st)
+{
+    if (ctas < 1) return cudaErrorInvalidValue;
+    k_level<<<ctas, kThreads, 0, st>>>(slots, tables, ctl, out);
+    return cudaGetLastError();
+}
+
+}  // namespace sbfs

@@ -11,6 +11,7 @@
 
 #include "classes.cuh"
 #include "common.cuh"
+#include "level.cuh"
 #include "sbfs.h"
 
 namespace sbfs {
@@ -64,6 +65,8 @@ struct Lane {
     cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr, ev_done = nullptr;
     DevBuf maps, ns, len, words, spill, order, counters, ranges, cta_queue, hbm_bitmap, hbm_queue,
         escal, tickets;
+    LevelEngine level;                         // device-resident slots for n > 20
+    bool level_ready = false;
     HostBuf h_counters;                        // pinned copy of DevCounters
     HostBuf h_maps, h_ns, h_len, h_words;      // pinned staging for pageable callers
     // chunk bookkeeping
@@ -82,6 +85,14 @@ struct Plan {
     CtaShape hbm;
 };
 
+}  // namespace sbfs
+
+struct sbfs_handle;
+
+namespace sbfs {
+sbfs_status engine_enqueue(sbfs_handle *h, Lane &L, const uint8_t *d_maps, int32_t lstride, const uint8_t *d_ns,
+                           int32_t n_uniform, int32_t max_n, int64_t count, int32_t *d_len, uint64_t *d_words,
+                           int32_t word_stride, int *launches);
 }  // namespace sbfs
 
 struct sbfs_handle {

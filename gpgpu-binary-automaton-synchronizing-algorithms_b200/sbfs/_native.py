@@ -19,6 +19,8 @@ EXPORTS = [
     "sbfs_status_string", "sbfs_best_parallelism", "sbfs_solve_batch", "sbfs_verify_batch",
     "sbfs_solve_plain", "sbfs_solve_batch_device", "sbfs_device_wait", "sbfs_host_alloc",
     "sbfs_host_free", "sbfs_word_stride", "sbfs_describe_plan", "sbfs_solve_small_noalloc",
+    "sbfs_server_config_default", "sbfs_server_start", "sbfs_server_submit", "sbfs_server_poll",
+    "sbfs_server_cancel", "sbfs_server_stats_get", "sbfs_server_reset_peak", "sbfs_server_stop",
 ]
 
 STATUS = {0: "SBFS_OK", 1: "SBFS_EINVAL", 2: "SBFS_ENOMEM", 3: "SBFS_ETIMEOUT", 4: "SBFS_ECUDA",
@@ -72,6 +74,38 @@ class Stats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int32),
+        ("max_batch", ctypes.c_int32),
+        ("max_levels", ctypes.c_int32),
+        ("queue_capacity", ctypes.c_int32),
+        ("arena_bytes", ctypes.c_int64),
+    ]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [
+        ("id", ctypes.c_uint64),
+        ("status", ctypes.c_int32),
+        ("len", ctypes.c_int32),
+        ("n", ctypes.c_int32),
+        ("pad", ctypes.c_int32),
+        ("word", ctypes.c_uint64 * 12),
+        ("submit_ms", ctypes.c_double),
+        ("done_ms", ctypes.c_double),
+    ]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int64) for k in (
+        "submitted", "completed", "rejected", "cancelled", "pending", "in_flight", "small_batches",
+        "level_launches", "arena_used", "arena_peak", "arena_capacity")] + [("now_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _lib: Optional[ctypes.CDLL] = None
 
 
@@ -117,6 +151,22 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.sbfs_host_alloc.restype = ctypes.c_int
     L.sbfs_solve_small_noalloc.argtypes = [P, i32, i32, i64, P, P, i32, P, P]
     L.sbfs_solve_small_noalloc.restype = ctypes.c_int
+    L.sbfs_server_config_default.argtypes = [ctypes.POINTER(ServerConfig)]
+    L.sbfs_server_config_default.restype = ctypes.c_int
+    L.sbfs_server_start.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(P)]
+    L.sbfs_server_start.restype = ctypes.c_int
+    L.sbfs_server_submit.argtypes = [P, P, P, i32, ctypes.POINTER(ctypes.c_uint64)]
+    L.sbfs_server_submit.restype = ctypes.c_int
+    L.sbfs_server_poll.argtypes = [P, ctypes.POINTER(Result), i32, ctypes.POINTER(i32), i32]
+    L.sbfs_server_poll.restype = ctypes.c_int
+    L.sbfs_server_cancel.argtypes = [P, ctypes.c_uint64]
+    L.sbfs_server_cancel.restype = ctypes.c_int
+    L.sbfs_server_stats_get.argtypes = [P, ctypes.POINTER(ServerStats)]
+    L.sbfs_server_stats_get.restype = ctypes.c_int
+    L.sbfs_server_reset_peak.argtypes = [P]
+    L.sbfs_server_reset_peak.restype = ctypes.c_int
+    L.sbfs_server_stop.argtypes = [P]
+    L.sbfs_server_stop.restype = ctypes.c_int
     L.sbfs_describe_plan.argtypes = [P, ctypes.c_char_p, i32]
     L.sbfs_describe_plan.restype = i32
     L.sbfs_host_free.argtypes = [P]

@@ -189,6 +189,63 @@ SBFS_API sbfs_status sbfs_solve_small_noalloc(const uint8_t *d_maps, int32_t lst
  * the full length needed. */
 SBFS_API int32_t sbfs_describe_plan(sbfs_handle *h, char *buf, int32_t len);
 
+/* ---------------------------------------------------------------------------
+ * Serving: a request loop on its own thread.  Requests (one automaton each)
+ * are admitted as they arrive: automata with n <= 16 are gathered into
+ * mini-batches and solved by the batch kernels; automata with n >= 17 are
+ * admitted into device-resident BFS slots while their 2^n-bit bitmap and
+ * queue fit the arena budget, and advance a few levels per launch alongside
+ * every other admitted request, so a request that arrives while others run is
+ * taken in as soon as memory frees up.  No reference counterpart (the
+ * reference solves fixed batches only, GPGPU/Program.cs:76-111).
+ * ------------------------------------------------------------------------- */
+typedef struct sbfs_server sbfs_server;
+
+typedef struct sbfs_server_config {
+    int32_t device;            /* CUDA device; -1 = current                                 */
+    int32_t max_batch;         /* small requests per mini-batch; 0 = 8192                   */
+    int32_t max_levels;        /* levels per launch batch of the large path; 0 = 16         */
+    int32_t queue_capacity;    /* pending requests before submit returns SBFS_EBUSY; 0 = 1<<20 */
+    int64_t arena_bytes;       /* HBM budget for admitted large requests; 0 = 16 GiB        */
+} sbfs_server_config;
+
+typedef struct sbfs_result {
+    uint64_t id;
+    int32_t status;            /* SBFS_OK or SBFS_ECANCELED                                 */
+    int32_t len;               /* -1 = not synchronizing                                    */
+    int32_t n;
+    int32_t pad;
+    uint64_t word[12];         /* letters as in sbfs_solve_batch (768 bits)                 */
+    double submit_ms;          /* server clock at submission                                */
+    double done_ms;            /* server clock when the result became available             */
+} sbfs_result;
+
+typedef struct sbfs_server_stats {
+    int64_t submitted, completed, rejected, cancelled;
+    int64_t pending;           /* submitted, not yet on the GPU                             */
+    int64_t in_flight;         /* on the GPU                                                */
+    int64_t small_batches, level_launches;
+    int64_t arena_used, arena_peak, arena_capacity;  /* bytes held by admitted large requests */
+    double now_ms;
+} sbfs_server_stats;
+
+SBFS_API sbfs_status sbfs_server_config_default(sbfs_server_config *cfg);
+SBFS_API sbfs_status sbfs_server_start(const sbfs_server_config *cfg, sbfs_server **out);
+/* Copies the automaton (a[0..n), b[0..n)); returns its id.  SBFS_EINVAL for a
+ * malformed automaton, SBFS_EBUSY when the pending queue is full. */
+SBFS_API sbfs_status sbfs_server_submit(sbfs_server *s, const uint8_t *a, const uint8_t *b, int32_t n,
+                                        uint64_t *out_id);
+/* Up to max finished results; waits up to timeout_ms for the first one. */
+SBFS_API sbfs_status sbfs_server_poll(sbfs_server *s, sbfs_result *out, int32_t max, int32_t *got,
+                                      int32_t timeout_ms);
+/* Cancels a pending request (its result comes back with SBFS_ECANCELED);
+ * SBFS_ENOTFOUND when it is unknown or already on the GPU. */
+SBFS_API sbfs_status sbfs_server_cancel(sbfs_server *s, uint64_t id);
+SBFS_API sbfs_status sbfs_server_stats_get(sbfs_server *s, sbfs_server_stats *out);
+SBFS_API sbfs_status sbfs_server_reset_peak(sbfs_server *s);
+/* Finishes everything submitted, then stops the loop and frees the server. */
+SBFS_API sbfs_status sbfs_server_stop(sbfs_server *s);
+
 /* uint64 per automaton needed for words of automata with at most max_n states:
  * ceil((max_n-1)^2 / 64), at least 1. */
 SBFS_API int32_t sbfs_word_stride(int32_t max_n);
