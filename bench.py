@@ -54,7 +54,9 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["sbfs", "reference"], default="sbfs")
-    ap.add_argument("--workload", choices=["n12", "n8", "mixed", "large"], default="n12")
+    ap.add_argument("--workload", choices=["n12", "n8", "mixed", "large", "serving"], default="n12")
+    ap.add_argument("--rates", default="2000,8000,32000,128000,0",
+                    help="serving: offered request rates per second (0 = submit all at once)")
     ap.add_argument("--count", type=int, default=0, help="automata per GPU (0 = the workload's size)")
     ap.add_argument("--cpu-seconds", type=float, default=1.5, help="wall time of the CPU baseline sample")
     ap.add_argument("--plain-sample", type=int, default=2000)
@@ -419,10 +421,109 @@ def run_sbfs(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# serving: open-loop Poisson arrivals of single-automaton requests
+# ---------------------------------------------------------------------------
+
+def run_serving(args):
+    import threading
+
+    import numpy as np
+
+    from sbfs import problem as P
+    from sbfs.server import Server
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    count = args.count or 20_000
+    seed = 0x5EED + 3
+    ns = P.log_uniform_sizes(count, 8, 24, seed)
+    recs = P.uniform_maps(count, ns, seed + 1)
+    cerny = np.arange(0, count, 20)          # 5% Cerny family
+    for i in cerny:
+        recs[i] = P.cerny_record(int(ns[i]))
+    a_rows = [np.ascontiguousarray(recs[i, :ns[i]]) for i in range(count)]
+    b_rows = [np.ascontiguousarray(recs[i, 32:32 + ns[i]]) for i in range(count)]
+    rates = [float(r) for r in args.rates.split(",")]
+    rng = np.random.default_rng(seed)
+    sweep = []
+    srv = Server(device=0)
+    # warm-up: every path once
+    warm = [srv.submit(a_rows[i], b_rows[i], int(ns[i])) for i in range(0, min(count, 2000), 7)]
+    srv.wait_all(warm)
+    for rate in rates:
+        srv.reset_peak()
+        gaps = rng.exponential(1.0 / rate, count) if rate > 0 else np.zeros(count)
+        times = np.cumsum(gaps)
+        ids = [0] * count
+        refused = [0]
+
+        def submitter():
+            t0 = time.perf_counter()
+            for i in range(count):
+                target = t0 + times[i]
+                while True:
+                    now = time.perf_counter()
+                    if now >= target:
+                        break
+                    if target - now > 2e-4:
+                        time.sleep((target - now) * 0.5)
+                while True:
+                    try:
+                        ids[i] = srv.submit(a_rows[i], b_rows[i], int(ns[i]))
+                        break
+                    except Exception:
+                        refused[0] += 1
+                        time.sleep(1e-4)
+
+        th = threading.Thread(target=submitter)
+        t_start = time.perf_counter()
+        th.start()
+        results = {}
+        while len(results) < count:
+            for r in srv.poll(timeout_ms=20):
+                results[r["id"]] = r
+            if not th.is_alive() and len(results) < count and time.perf_counter() - t_start > 600:
+                raise SystemExit("serving run did not finish")
+        th.join()
+        wall = time.perf_counter() - t_start
+        st = srv.stats()
+        by_id = [results[i] for i in ids]
+        lat = np.array([r["done_ms"] - r["submit_ms"] for r in by_id])
+        small = np.array([int(r["n"]) <= 20 for r in by_id])
+        first = min(r["submit_ms"] for r in by_id)
+        last = max(r["done_ms"] for r in by_id)
+        entry = {
+            "offered_per_s": rate if rate > 0 else "all at once",
+            "achieved_automata_per_s": count / ((last - first) / 1e3),
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                           "max": float(lat.max())},
+            "latency_ms_n_le_20": {"p50": float(np.percentile(lat[small], 50)),
+                                   "p99": float(np.percentile(lat[small], 99))},
+            "peak_arena_bytes": int(st["arena_peak"]), "submit_retries": refused[0], "wall_s": wall,
+        }
+        sweep.append(entry)
+        print(json.dumps({"serving_rate": entry}), file=sys.stderr, flush=True)
+    srv.stop()
+    best = max(sweep, key=lambda e: e["achieved_automata_per_s"])
+    line = {
+        "metric": METRIC, "value": best["achieved_automata_per_s"], "unit": UNIT, "n_gpus": 1, "steps": len(rates),
+        "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u16", "data": "synthetic",
+        "config": {"workload": f"serving: {count:,} single-automaton requests, n log-uniform 8..24, 5% Cerny, "
+                               "open-loop Poisson arrivals at swept rates", "rates": args.rates},
+        "serving": sweep,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "serving":
+        return run_serving(args)
     return run_sbfs(args)
 
 
