@@ -61,6 +61,7 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=1.5, help="wall time of the CPU baseline sample")
     ap.add_argument("--plain-sample", type=int, default=2000)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default kernel shapes")
     return ap.parse_args()
 
 
@@ -252,8 +253,10 @@ def run_sbfs(args):
     wl = make_workload(args.workload, args.count, rank)
     count, lstride = wl["count"], wl["lstride"]
     ws = sbfs.word_stride_for(wl["max_n"])
-    eng = sbfs.Engine(device=dev.index)
-    plan = eng.plan()
+    import tempfile
+    tune_cache = os.path.join(tempfile.gettempdir(), "sbfs_tune_cache.txt")
+    eng = sbfs.Engine(device=dev.index, autotune=not args.no_tune, tune_cache=tune_cache)
+    plan = eng.plan()   # runs the autotuner (or reads its cache) before any timing
 
     def barrier():
         if dist:

@@ -202,7 +202,7 @@ sbfs_status run_level_class(sbfs_handle *h, Lane &L, const Job &j, const Batch &
     while (next < items.size() || E.in_flight() > 0) {
         while (next < items.size()) {
             const int n = items[next].second;
-            if (n < 21 || n > SBFS_MAX_N) return fail(h, SBFS_EINVAL, "n out of range for the level class");
+            if (n < 1 || n > SBFS_MAX_N) return fail(h, SBFS_EINVAL, "n out of range");
             if (E.admit(j.maps + (size_t)items[next].first * rec, j.lstride, n, items[next].first, nullptr,
                         nullptr) < 0)
                 break;
@@ -261,7 +261,7 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
         Batch bc = b;
         if (j.ns) bc.range_dev = L.ranges.as<unsigned long long>() + kNumClasses + 2 * c;
         unsigned long long *ticket = ticket_override ? ticket_override : &ctr->ticket[c];
-        if (c < 2 && !plain && h->cfg.small_kernel != 2) {
+        if (c < 2 && !plain && !P.use_pool[c]) {
             const LaneShape &ls = P.lane[c];
             CK(L.escal.reserve((size_t)std::max<int64_t>(j.count, 1) * sizeof(int32_t)), "allocating escalation list");
             CK(launch_lane(ls.nmax, ls.warps, ls.ring, ls.refill_k, ls.ctas, bc, L.escal.as<int32_t>(),
@@ -271,6 +271,10 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
             const PoolShape &s = P.pool[c];
             CK(L.spill.reserve(pool_spill_words(s) * sizeof(uint32_t)), "allocating queue spill");
             CK(launch_pool(s, bc, L.spill.as<uint32_t>(), ticket, st), "launching small-n kernel");
+        } else if (c == 3 && P.class3_level && !plain) {
+            sbfs_status ls = run_level_class(h, L, j, bc, launches);
+            if (ls) return ls;
+            continue;
         } else if (c == 3) {
             const int nb = std::min(20, std::max(j.ns ? j.max_n : j.n_uniform, 17));
             const int per_sm = cta_max_ctas_per_sm(nb, P.cta.threads);
@@ -286,7 +290,8 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
         }
         *launches += 1;
     }
-    if (!plain && (present & 3) && h->cfg.small_kernel != 2) {
+    const bool lane_used = ((present & 1) && !P.use_pool[0]) || ((present & 2) && !P.use_pool[1]);
+    if (!plain && lane_used) {
         // automata the per-lane kernel handed back (frontier wider than its ring,
         // or a word longer than an entry carries) go through the pooled kernel
         Batch be = b;
@@ -354,11 +359,17 @@ sbfs_status ensure_plan(sbfs_handle *h)
     P.cta.ctas = sms * 4;
     P.hbm.threads = 512;
     P.hbm.ctas = sms * 4;
+    P.use_pool[0] = P.use_pool[1] = h->cfg.small_kernel == 2 ? 1 : 0;
+    P.class3_level = 0;
+    P.tuned = 0;
+    h->plan_ready = true;   // the tuner below runs batches with the defaults in place
     if (h->cfg.autotune) {
         cudaError_t e = plan_autotune(h, P);
-        if (e != cudaSuccess) return cuda_fail(h, e, "autotuning kernel shapes");
+        if (e != cudaSuccess) {
+            h->plan_ready = false;
+            return cuda_fail(h, e, "autotuning kernel shapes");
+        }
     }
-    h->plan_ready = true;
     return SBFS_OK;
 }
 
@@ -815,12 +826,12 @@ int32_t sbfs_describe_plan(sbfs_handle *h, char *buf, int32_t len)
         return 0;
     }
     const Plan &P = h->plan;
-    std::string js = "{\"small_kernel\":\"";
-    js += h->cfg.small_kernel == 2 ? "pool" : "lane";
-    js += "\",\"classes\":[";
+    std::string js = "{\"tuned\":";
+    js += P.tuned ? "true" : "false";
+    js += ",\"classes\":[";
     char tmp[256];
     for (int c = 0; c < 3; ++c) {
-        const bool lane = c < 2 && h->cfg.small_kernel != 2;
+        const bool lane = c < 2 && !P.use_pool[c];
         if (lane) {
             const LaneShape &l = P.lane[c];
             std::snprintf(tmp, sizeof tmp,
@@ -837,9 +848,9 @@ int32_t sbfs_describe_plan(sbfs_handle *h, char *buf, int32_t len)
         js += tmp;
     }
     std::snprintf(tmp, sizeof tmp,
-                  "{\"class\":3,\"max_n\":20,\"kernel\":\"k_cta\",\"threads\":%d,\"ctas\":%d},"
+                  "{\"class\":3,\"max_n\":20,\"kernel\":\"%s\",\"threads\":%d,\"ctas\":%d},"
                   "{\"class\":4,\"max_n\":28,\"kernel\":\"k_level\",\"threads\":512,\"slots\":%d}]}",
-                  P.cta.threads, P.cta.ctas, kMaxLevelSlots);
+                  P.class3_level ? "k_level" : "k_cta", P.cta.threads, P.cta.ctas, kMaxLevelSlots);
     js += tmp;
     if (buf && len > 0) {
         std::strncpy(buf, js.c_str(), (size_t)len - 1);

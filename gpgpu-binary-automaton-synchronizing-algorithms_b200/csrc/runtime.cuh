@@ -83,6 +83,9 @@ struct Plan {
     PoolShape pool[3];
     CtaShape cta;
     CtaShape hbm;
+    int use_pool[2];     // classes 0, 1: 1 = warp-pooled kernel instead of one automaton per lane
+    int class3_level;    // class 3: 1 = bitmaps in HBM (level slots) instead of shared memory (k_cta)
+    int tuned;           // 1 when the autotuner (or its cache) chose the shapes
 };
 
 }  // namespace sbfs

@@ -1,12 +1,297 @@
-// tune.cu -- kernel-shape autotuner (placeholder: keeps the defaults).
+// tune.cu -- kernel-shape autotuner.
+//
+// For each size class the tuner generates a synthetic batch of uniform random
+// automata of the class's largest n on the device (no host copies), times the
+// candidate kernels and shapes on it with CUDA events (best of two runs after
+// a warm-up), and keeps the fastest:
+//   classes 0, 1 (n <= 8, n <= 12): one automaton per lane (warps per CTA,
+//                 frontier ring, refill threshold) vs the warp-pooled kernel
+//                 (automata per warp, warps per CTA, on-chip queue entries);
+//   class 2 (n <= 16): warp-pooled shapes;
+//   class 3 (n <= 20): bitmap placement -- shared memory (one automaton per
+//                 CTA, threads per CTA) vs HBM (device-resident level slots).
+// The choice is cached per device (name, SM count, library version) in the
+// file named by sbfs_config.tune_cache, so later handles skip the measurement.
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
 #include "runtime.cuh"
 
 namespace sbfs {
+namespace {
+
+__global__ void k_gen(uint8_t *recs, int lstride, int n, int64_t count, unsigned long long seed)
+{
+    const int64_t bytes = count * 2 * lstride;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < bytes; i += (int64_t)gridDim.x * blockDim.x) {
+        const int j = (int)(i % (2 * lstride));
+        const int st = j % lstride;
+        unsigned long long z = seed + (unsigned long long)i * 0x9E3779B97F4A7C15ull;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        recs[i] = st < n ? (uint8_t)(((z >> 32) * (unsigned long long)n) >> 32) : 0;
+    }
+}
+
+struct Bench {
+    sbfs_handle *h;
+    Lane *L;
+    DevBuf recs, len, words;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+};
+
+cudaError_t prepare(Bench &b, int n, int64_t count)
+{
+    cudaError_t e;
+    if ((e = b.recs.reserve((size_t)count * 64)) != cudaSuccess) return e;
+    if ((e = b.len.reserve((size_t)count * 4)) != cudaSuccess) return e;
+    if ((e = b.words.reserve((size_t)count * 8 * 6)) != cudaSuccess) return e;
+    k_gen<<<1024, 256, 0, b.L->stream>>>(b.recs.as<uint8_t>(), 32, n, count, 0x5EEDull + (unsigned)n);
+    return cudaGetLastError();
+}
+
+// milliseconds of one solve of the prepared batch with the handle's current plan
+double time_plan(Bench &b, int n, int64_t count)
+{
+    const int ws = sbfs_word_stride(n);
+    double best = 1e30;
+    for (int rep = 0; rep < 3; ++rep) {
+        int launches = 0;
+        cudaEventRecord(b.e0, b.L->stream);
+        sbfs_status s = engine_enqueue(b.h, *b.L, b.recs.as<uint8_t>(), 32, nullptr, n, n, count,
+                                       b.len.as<int32_t>(), b.words.as<uint64_t>(), ws, &launches);
+        cudaEventRecord(b.e1, b.L->stream);
+        if (s != SBFS_OK || cudaEventSynchronize(b.e1) != cudaSuccess) {
+            cudaGetLastError();
+            return 1e30;
+        }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, b.e0, b.e1);
+        if (rep > 0 && ms < best) best = ms;   // rep 0 is the warm-up
+    }
+    return best;
+}
+
+std::string device_key(sbfs_handle *h)
+{
+    cudaDeviceProp p;
+    cudaGetDeviceProperties(&p, h->device);
+    char buf[256];
+    std::snprintf(buf, sizeof buf, "%s|sm%d|abi%d|v2", p.name, h->sm_count, SBFS_ABI_VERSION);
+    for (char *c = buf; *c; ++c)
+        if (*c == ' ') *c = '_';
+    return buf;
+}
+
+std::string encode(const Plan &P)
+{
+    char buf[512];
+    std::snprintf(buf, sizeof buf,
+                  "c0=%d,%d,%d,%d,%d,%d,%d c1=%d,%d,%d,%d,%d,%d,%d c2=%d,%d,%d c3=%d,%d",
+                  P.use_pool[0], P.lane[0].warps, P.lane[0].ring, P.lane[0].refill_k, P.pool[0].slots, P.pool[0].warps,
+                  P.pool[0].queue_smem, P.use_pool[1], P.lane[1].warps, P.lane[1].ring, P.lane[1].refill_k,
+                  P.pool[1].slots, P.pool[1].warps, P.pool[1].queue_smem, P.pool[2].slots, P.pool[2].warps,
+                  P.pool[2].queue_smem, P.class3_level, P.cta.threads);
+    return buf;
+}
+
+bool decode(const char *s, Plan &P)
+{
+    Plan Q = P;
+    const int got = std::sscanf(
+        s, "c0=%d,%d,%d,%d,%d,%d,%d c1=%d,%d,%d,%d,%d,%d,%d c2=%d,%d,%d c3=%d,%d", &Q.use_pool[0], &Q.lane[0].warps,
+        &Q.lane[0].ring, &Q.lane[0].refill_k, &Q.pool[0].slots, &Q.pool[0].warps, &Q.pool[0].queue_smem,
+        &Q.use_pool[1], &Q.lane[1].warps, &Q.lane[1].ring, &Q.lane[1].refill_k, &Q.pool[1].slots, &Q.pool[1].warps,
+        &Q.pool[1].queue_smem, &Q.pool[2].slots, &Q.pool[2].warps, &Q.pool[2].queue_smem, &Q.class3_level,
+        &Q.cta.threads);
+    if (got != 19) return false;
+    P = Q;
+    return true;
+}
+
+// grid sizes follow from the shapes and the occupancy of this device
+bool finish_shapes(sbfs_handle *h, Plan &P)
+{
+    for (int c = 0; c < 2; ++c) {
+        const int per = lane_max_ctas_per_sm(P.lane[c].nmax, P.lane[c].warps, P.lane[c].ring);
+        if (per < 1) return false;
+        P.lane[c].ctas = per * h->sm_count;
+    }
+    for (int c = 0; c < 3; ++c) {
+        PoolShape s = P.pool[c];
+        s.ctas = 1;
+        const int per = pool_max_ctas_per_sm(s);
+        if (per < 1) return false;
+        P.pool[c].ctas = per * h->sm_count;
+    }
+    return true;
+}
+
+bool load_cache(const char *path, const std::string &key, Plan &P)
+{
+    if (!path) return false;
+    FILE *f = std::fopen(path, "r");
+    if (!f) return false;
+    char line[1024];
+    bool ok = false;
+    while (std::fgets(line, sizeof line, f)) {
+        const size_t kl = key.size();
+        if (std::strncmp(line, key.c_str(), kl) == 0 && line[kl] == ' ') ok = decode(line + kl + 1, P);
+    }
+    std::fclose(f);
+    return ok;
+}
+
+void store_cache(const char *path, const std::string &key, const Plan &P)
+{
+    if (!path) return;
+    std::vector<std::string> keep;
+    if (FILE *f = std::fopen(path, "r")) {
+        char line[1024];
+        while (std::fgets(line, sizeof line, f))
+            if (std::strncmp(line, key.c_str(), key.size()) != 0) keep.push_back(line);
+        std::fclose(f);
+    }
+    if (FILE *f = std::fopen(path, "w")) {
+        for (auto &l : keep) std::fputs(l.c_str(), f);
+        std::fprintf(f, "%s %s\n", key.c_str(), encode(P).c_str());
+        std::fclose(f);
+    }
+}
+
+}  // namespace
 
 cudaError_t plan_autotune(sbfs_handle *h, Plan &plan)
 {
-    (void)h;
-    (void)plan;
+    // `plan` is the handle's own plan, which every candidate run overwrites: work on a copy
+    Plan P = plan;
+    const std::string key = device_key(h);
+    Plan cached = P;
+    if (load_cache(h->cfg.tune_cache, key, cached) && finish_shapes(h, cached)) {
+        cached.tuned = 1;
+        h->plan = cached;
+        return cudaSuccess;
+    }
+    Bench b;
+    b.h = h;
+    b.L = &h->lanes[0];
+    cudaError_t e;
+    if ((e = cudaEventCreate(&b.e0)) != cudaSuccess || (e = cudaEventCreate(&b.e1)) != cudaSuccess) return e;
+
+    // ---- classes 0 and 1: per-lane vs warp-pooled --------------------------
+    for (int c = 0; c < 2; ++c) {
+        const int n = kClassMaxN[c];
+        const int64_t count = 1 << 18;
+        if ((e = prepare(b, n, count)) != cudaSuccess) break;
+        Plan best = P;
+        double best_ms = 1e30;
+        const int warps_c[2][3] = {{2, 4, 8}, {1, 2, 0}};
+        for (int w : warps_c[c])
+            for (int ring : {16, 32, 64})
+                for (int rk : {8, 16}) {
+                    if (!w) continue;
+                    Plan t = P;
+                    t.use_pool[c] = 0;
+                    t.lane[c].warps = w;
+                    t.lane[c].ring = ring;
+                    t.lane[c].refill_k = rk;
+                    const int per = lane_max_ctas_per_sm(n, w, ring);
+                    if (per < 1) continue;
+                    t.lane[c].ctas = per * h->sm_count;
+                    h->plan = t;
+                    const double ms = time_plan(b, n, count);
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        best = t;
+                    }
+                }
+        for (int S : {4, 8, 16})
+            for (int W : {1, 2, 4})
+                for (int Q : {64, 128}) {
+                    Plan t = P;
+                    t.use_pool[c] = 1;
+                    t.pool[c].slots = S;
+                    t.pool[c].warps = W;
+                    t.pool[c].queue_smem = Q;
+                    PoolShape s = t.pool[c];
+                    s.ctas = 1;
+                    const int per = pool_max_ctas_per_sm(s);
+                    if (per < 1) continue;
+                    t.pool[c].ctas = per * h->sm_count;
+                    h->plan = t;
+                    const double ms = time_plan(b, n, count);
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        best = t;
+                    }
+                }
+        P.use_pool[c] = best.use_pool[c];
+        P.lane[c] = best.lane[c];
+        P.pool[c] = best.pool[c];
+    }
+    // ---- class 2: pooled shapes ---------------------------------------------
+    if (e == cudaSuccess && (e = prepare(b, 16, 1 << 16)) == cudaSuccess) {
+        Plan best = P;
+        double best_ms = 1e30;
+        for (int S : {2, 4, 8})
+            for (int W : {1, 2})
+                for (int Q : {128, 256, 512}) {
+                    Plan t = P;
+                    t.pool[2].slots = S;
+                    t.pool[2].warps = W;
+                    t.pool[2].queue_smem = Q;
+                    PoolShape s = t.pool[2];
+                    s.ctas = 1;
+                    const int per = pool_max_ctas_per_sm(s);
+                    if (per < 1 || (S == 2)) continue;   // 2 slots per warp is not instantiated
+                    t.pool[2].ctas = per * h->sm_count;
+                    h->plan = t;
+                    const double ms = time_plan(b, 16, 1 << 16);
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        best = t;
+                    }
+                }
+        P.pool[2] = best.pool[2];
+    }
+    // ---- class 3: shared-memory bitmaps (per CTA) vs HBM bitmaps (level slots)
+    if (e == cudaSuccess && (e = prepare(b, 20, 1 << 13)) == cudaSuccess) {
+        Plan best = P;
+        double best_ms = 1e30;
+        for (int threads : {256, 512, 1024}) {
+            Plan t = P;
+            t.class3_level = 0;
+            t.cta.threads = threads;
+            h->plan = t;
+            const double ms = time_plan(b, 20, 1 << 13);
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = t;
+            }
+        }
+        Plan t = P;
+        t.class3_level = 1;
+        h->plan = t;
+        const double ms = time_plan(b, 20, 1 << 13);
+        if (ms < best_ms) best = t;
+        P.class3_level = best.class3_level;
+        P.cta = best.cta;
+    }
+    cudaEventDestroy(b.e0);
+    cudaEventDestroy(b.e1);
+    b.recs.release();
+    b.len.release();
+    b.words.release();
+    if (e != cudaSuccess) {
+        h->plan = P;
+        return e;
+    }
+    P.tuned = 1;
+    h->plan = P;
+    store_cache(h->cfg.tune_cache, key, P);
     return cudaSuccess;
 }
 
