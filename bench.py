@@ -62,6 +62,7 @@ def parse_args():
     ap.add_argument("--plain-sample", type=int, default=2000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default kernel shapes")
+    ap.add_argument("--no-graph", action="store_true", help="launch every step directly, no CUDA graphs")
     return ap.parse_args()
 
 
@@ -255,7 +256,8 @@ def run_sbfs(args):
     ws = sbfs.word_stride_for(wl["max_n"])
     import tempfile
     tune_cache = os.path.join(tempfile.gettempdir(), "sbfs_tune_cache.txt")
-    eng = sbfs.Engine(device=dev.index, autotune=not args.no_tune, tune_cache=tune_cache)
+    eng = sbfs.Engine(device=dev.index, autotune=not args.no_tune, tune_cache=tune_cache,
+                      use_graph=not args.no_graph)
     plan = eng.plan()   # runs the autotuner (or reads its cache) before any timing
 
     def barrier():

@@ -432,6 +432,70 @@ sbfs_status finish_lane(sbfs_handle *h, Lane &L, Totals &t)
     return SBFS_OK;
 }
 
+// Runs `body` (stream work on L.stream) directly, or replays it from a CUDA
+// graph.  A key's first run is direct (it sizes the lane's buffers); its second
+// run is captured; later runs launch the graph.  A graph whose lane buffers
+// moved since capture is rebuilt.
+template <class F>
+sbfs_status run_maybe_captured(sbfs_handle *h, Lane &L, const std::string &key, bool allow, int *launches, F &&body)
+{
+    if (!allow) return body();
+    auto it = L.graphs.find(key);
+    if (it != L.graphs.end()) {
+        if (it->second.sig == L.signature()) {
+            CK(cudaGraphLaunch(it->second.exec, L.stream), "launching graph");
+            *launches += it->second.launches;
+            return SBFS_OK;
+        }
+        cudaGraphExecDestroy(it->second.exec);
+        L.graphs.erase(it);
+    }
+    if (!L.seen.count(key)) {
+        L.seen.insert(key);
+        return body();
+    }
+    const uint64_t sig = L.signature();
+    const int before = *launches;
+    CK(cudaStreamBeginCapture(L.stream, cudaStreamCaptureModeThreadLocal), "beginning capture");
+    const sbfs_status s = body();
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(L.stream, &g);
+    if (s != SBFS_OK || e != cudaSuccess || L.signature() != sig) {
+        // not capturable this time (or it reallocated): run it directly instead
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        *launches = before;
+        return body();
+    }
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ie = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+        cudaGetLastError();
+        *launches = before;
+        return body();
+    }
+    if (L.graphs.size() >= 64) L.drop_graphs();
+    L.graphs[key] = {exec, sig, *launches - before};
+    CK(cudaGraphLaunch(exec, L.stream), "launching graph");
+    return SBFS_OK;
+}
+
+// Launch sequences that never wait on the host (no level-slot classes) can be captured.
+bool graph_safe(sbfs_handle *h, int max_n)
+{
+    return max_n <= kClassMaxN[2] || (max_n <= kClassMaxN[3] && !h->plan.class3_level);
+}
+
+std::string graph_key(const void *a, const void *b, const void *c, const void *d, const void *e, int64_t cnt,
+                      int lstride, int n_uniform, int max_n, int ws)
+{
+    char buf[256];
+    std::snprintf(buf, sizeof buf, "%p|%p|%p|%p|%p|%lld|%d|%d|%d|%d", a, b, c, d, e, (long long)cnt, lstride,
+                  n_uniform, max_n, ws);
+    return buf;
+}
+
 sbfs_status solve_host(sbfs_handle *h, const uint8_t *maps, int32_t lstride, const uint8_t *ns,
                        int32_t n_uniform, int64_t count, int32_t *out_len, uint64_t *out_words,
                        int32_t word_stride, int64_t *out_first_violation, sbfs_stats *stats, bool plain)
@@ -480,25 +544,65 @@ sbfs_status solve_host(sbfs_handle *h, const uint8_t *maps, int32_t lstride, con
                 src_ns = L.h_ns.as<uint8_t>();
             }
         }
-        CK(cudaMemcpyAsync(L.maps.ptr, src_maps, cnt * rec, cudaMemcpyHostToDevice, L.stream), "copying records");
-        h2d += cnt * rec;
-        if (ns) {
-            CK(cudaMemcpyAsync(L.ns.ptr, src_ns, cnt, cudaMemcpyHostToDevice, L.stream), "copying sizes");
-            h2d += cnt;
+        L.staged_out = !pin_out;
+        L.user_len = out_len;
+        L.user_words = out_words;
+        L.word_stride = word_stride;
+        void *dst_len = nullptr, *dst_words = nullptr;
+        const size_t wb = out_words ? (size_t)cnt * word_stride * sizeof(uint64_t) : 0;
+        if (out_len) {
+            dst_len = pin_out ? (void *)(out_len + begin) : nullptr;
+            if (!pin_out) {
+                CK(L.h_len.reserve(cnt * sizeof(int32_t)), "allocating pinned staging");
+                dst_len = L.h_len.ptr;
+            }
         }
-        if ((s = reset_counters(h, L))) return s;
+        if (out_words) {
+            dst_words = pin_out ? (void *)(out_words + (size_t)begin * word_stride) : nullptr;
+            if (!pin_out) {
+                CK(L.h_words.reserve(wb), "allocating pinned staging");
+                dst_words = L.h_words.ptr;
+            }
+        }
         Job j{L.maps.as<uint8_t>(), lstride, ns ? L.ns.as<uint8_t>() : nullptr, n_uniform, max_n, cnt,
               out_len ? L.len.as<int32_t>() : nullptr, out_words ? L.words.as<uint64_t>() : nullptr,
               word_stride};
+        h2d += cnt * rec + (ns ? cnt : 0);
+        d2h += (out_len ? cnt * (int64_t)sizeof(int32_t) : 0) + (int64_t)wb;
         CK(cudaEventRecord(L.ev_k0, L.stream), "recording event");
         if (!plain) {
-            if ((s = enqueue_kernels(h, L, j, &launches))) return s;
+            // one chunk: copies in, counters, bucketing, class kernels, copies out
+            auto body = [&]() -> sbfs_status {
+                CK(cudaMemcpyAsync(L.maps.ptr, src_maps, cnt * rec, cudaMemcpyHostToDevice, L.stream),
+                   "copying records");
+                if (ns) CK(cudaMemcpyAsync(L.ns.ptr, src_ns, cnt, cudaMemcpyHostToDevice, L.stream), "copying sizes");
+                sbfs_status bs = reset_counters(h, L);
+                if (bs) return bs;
+                if ((bs = enqueue_kernels(h, L, j, &launches))) return bs;
+                if (out_len)
+                    CK(cudaMemcpyAsync(dst_len, L.len.ptr, cnt * sizeof(int32_t), cudaMemcpyDeviceToHost, L.stream),
+                       "copying lengths");
+                if (out_words)
+                    CK(cudaMemcpyAsync(dst_words, L.words.ptr, wb, cudaMemcpyDeviceToHost, L.stream), "copying words");
+                CK(cudaMemcpyAsync(L.h_counters.ptr, L.counters.ptr, sizeof(DevCounters), cudaMemcpyDeviceToHost,
+                                   L.stream),
+                   "copying counters");
+                return SBFS_OK;
+            };
+            const bool graphable = h->cfg.use_graph && graph_safe(h, max_n);
+            const std::string key = graphable ? graph_key(src_maps, src_ns, dst_len, dst_words, nullptr, cnt, lstride,
+                                                          n_uniform, max_n, word_stride)
+                                              : std::string();
+            if ((s = run_maybe_captured(h, L, key, graphable, &launches, body))) return s;
+            CK(cudaEventRecord(L.ev_k1, L.stream), "recording event");
         } else {
+            CK(cudaMemcpyAsync(L.maps.ptr, src_maps, cnt * rec, cudaMemcpyHostToDevice, L.stream), "copying records");
+            if (ns) CK(cudaMemcpyAsync(L.ns.ptr, src_ns, cnt, cudaMemcpyHostToDevice, L.stream), "copying sizes");
+            if ((s = reset_counters(h, L))) return s;
             // one launch per automaton, same kernels, one-CTA grid
             Plan saved = h->plan;
             for (int c = 0; c < 3; ++c) h->plan.pool[c].ctas = 1;
             h->plan.cta.ctas = 1;
-            h->plan.hbm.ctas = h->sm_count;   // the HBM kernel is grid-wide by construction
             CK(L.tickets.reserve((size_t)cnt * sizeof(unsigned long long)), "allocating tickets");
             CK(cudaMemsetAsync(L.tickets.ptr, 0, (size_t)cnt * sizeof(unsigned long long), L.stream),
                "resetting tickets");
@@ -522,35 +626,16 @@ sbfs_status solve_host(sbfs_handle *h, const uint8_t *maps, int32_t lstride, con
                 }
             }
             h->plan = saved;
+            CK(cudaEventRecord(L.ev_k1, L.stream), "recording event");
+            if (out_len)
+                CK(cudaMemcpyAsync(dst_len, L.len.ptr, cnt * sizeof(int32_t), cudaMemcpyDeviceToHost, L.stream),
+                   "copying lengths");
+            if (out_words)
+                CK(cudaMemcpyAsync(dst_words, L.words.ptr, wb, cudaMemcpyDeviceToHost, L.stream), "copying words");
+            CK(cudaMemcpyAsync(L.h_counters.ptr, L.counters.ptr, sizeof(DevCounters), cudaMemcpyDeviceToHost,
+                               L.stream),
+               "copying counters");
         }
-        CK(cudaEventRecord(L.ev_k1, L.stream), "recording event");
-        L.staged_out = !pin_out;
-        L.user_len = out_len;
-        L.user_words = out_words;
-        L.word_stride = word_stride;
-        if (out_len) {
-            void *dst = pin_out ? (void *)(out_len + begin) : nullptr;
-            if (!pin_out) {
-                CK(L.h_len.reserve(cnt * sizeof(int32_t)), "allocating pinned staging");
-                dst = L.h_len.ptr;
-            }
-            CK(cudaMemcpyAsync(dst, L.len.ptr, cnt * sizeof(int32_t), cudaMemcpyDeviceToHost, L.stream),
-               "copying lengths");
-            d2h += cnt * sizeof(int32_t);
-        }
-        if (out_words) {
-            const size_t wb = (size_t)cnt * word_stride * sizeof(uint64_t);
-            void *dst = pin_out ? (void *)(out_words + (size_t)begin * word_stride) : nullptr;
-            if (!pin_out) {
-                CK(L.h_words.reserve(wb), "allocating pinned staging");
-                dst = L.h_words.ptr;
-            }
-            CK(cudaMemcpyAsync(dst, L.words.ptr, wb, cudaMemcpyDeviceToHost, L.stream), "copying words");
-            d2h += wb;
-        }
-        CK(cudaMemcpyAsync(L.h_counters.ptr, L.counters.ptr, sizeof(DevCounters), cudaMemcpyDeviceToHost,
-                           L.stream),
-           "copying counters");
         CK(cudaEventRecord(L.ev_done, L.stream), "recording event");
         L.busy = true;
         L.begin = begin;
@@ -676,6 +761,7 @@ sbfs_status sbfs_destroy(sbfs_handle *h)
     cudaSetDevice(h->device);
     for (auto &L : h->lanes) {
         if (L.stream) cudaStreamSynchronize(L.stream);
+        L.drop_graphs();
         for (DevBuf *d : {&L.maps, &L.ns, &L.len, &L.words, &L.spill, &L.order, &L.counters, &L.ranges,
                           &L.cta_queue, &L.hbm_bitmap, &L.hbm_queue, &L.escal, &L.tickets})
             d->release();
@@ -764,26 +850,30 @@ sbfs_status sbfs_solve_batch_device(sbfs_handle *h, const uint8_t *d_maps, int32
     CK(L.h_counters.reserve(sizeof(DevCounters)), "allocating pinned counters");
     cudaStream_t saved = L.stream;
     L.stream = st;
-    if ((s = reset_counters(h, L))) {
-        L.stream = saved;
-        return s;
-    }
     Job j{d_maps, lstride, d_ns, n_uniform, d_ns ? (max_n > 0 ? std::min(max_n, SBFS_MAX_N) : SBFS_MAX_N) : n_uniform,
           count, d_len, d_words, d_words ? word_stride : 0};
     int launches = 0;
-    CK(cudaEventRecord(h->ev_dk0, st), "recording event");
-    if (count > 0) s = enqueue_kernels(h, L, j, &launches);
-    if (!s) {
+    // counters, bucketing, class kernels, the violation index, counters back to the host
+    auto body = [&]() -> sbfs_status {
+        sbfs_status bs = reset_counters(h, L);
+        if (bs) return bs;
+        if (count > 0 && (bs = enqueue_kernels(h, L, j, &launches))) return bs;
         launches += 1;
-        finalize_violation<<<1, 1, 0, st>>>(L.counters.as<DevCounters>(), d_first_violation);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) s = cuda_fail(h, e, "launching finalize");
-    }
+        finalize_violation<<<1, 1, 0, L.stream>>>(L.counters.as<DevCounters>(), d_first_violation);
+        CK(cudaGetLastError(), "launching finalize");
+        CK(cudaMemcpyAsync(L.h_counters.ptr, L.counters.ptr, sizeof(DevCounters), cudaMemcpyDeviceToHost, L.stream),
+           "copying counters");
+        return SBFS_OK;
+    };
+    const bool graphable = h->cfg.use_graph && graph_safe(h, j.max_n);
+    const std::string key = graphable ? graph_key(d_maps, d_ns, d_len, d_words, d_first_violation, count, lstride,
+                                                  n_uniform, j.max_n, word_stride)
+                                      : std::string();
+    CK(cudaEventRecord(h->ev_dk0, st), "recording event");
+    s = run_maybe_captured(h, L, key, graphable, &launches, body);
     L.stream = saved;
     if (s) return s;
     CK(cudaEventRecord(h->ev_dk1, st), "recording event");
-    CK(cudaMemcpyAsync(L.h_counters.ptr, L.counters.ptr, sizeof(DevCounters), cudaMemcpyDeviceToHost, st),
-       "copying counters");
     CK(cudaEventRecord(h->ev_device, st), "recording event");
     if (st != L.stream) CK(cudaStreamWaitEvent(L.stream, h->ev_device, 0), "ordering streams");
     h->device_pending = true;

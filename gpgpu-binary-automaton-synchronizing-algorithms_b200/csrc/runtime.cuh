@@ -3,7 +3,9 @@
 #pragma once
 
 #include <cstdint>
+#include <map>
 #include <mutex>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -76,6 +78,31 @@ struct Lane {
     int32_t *user_len = nullptr;
     uint64_t *user_words = nullptr;
     int32_t word_stride = 0;
+    // CUDA graphs of launch sequences already seen on this lane, keyed by their
+    // pointers and sizes; `sig` is the lane's buffer addresses at capture time
+    struct Graph {
+        cudaGraphExec_t exec;
+        uint64_t sig;
+        int launches;
+    };
+    std::map<std::string, Graph> graphs;
+    std::set<std::string> seen;
+    uint64_t signature() const
+    {
+        uint64_t x = 1469598103934665603ull;
+        for (const DevBuf *d : {&maps, &ns, &len, &words, &spill, &order, &counters, &ranges, &cta_queue, &escal,
+                                &tickets})
+            x = (x ^ reinterpret_cast<uint64_t>(d->ptr)) * 1099511628211ull;
+        for (const HostBuf *b : {&h_counters, &h_maps, &h_ns, &h_len, &h_words})
+            x = (x ^ reinterpret_cast<uint64_t>(b->ptr)) * 1099511628211ull;
+        return x;
+    }
+    void drop_graphs()
+    {
+        for (auto &g : graphs) cudaGraphExecDestroy(g.second.exec);
+        graphs.clear();
+        seen.clear();
+    }
 };
 
 struct Plan {

@@ -80,7 +80,7 @@ std::string device_key(sbfs_handle *h)
     cudaDeviceProp p;
     cudaGetDeviceProperties(&p, h->device);
     char buf[256];
-    std::snprintf(buf, sizeof buf, "%s|sm%d|abi%d|v2", p.name, h->sm_count, SBFS_ABI_VERSION);
+    std::snprintf(buf, sizeof buf, "%s|sm%d|abi%d|v3", p.name, h->sm_count, SBFS_ABI_VERSION);
     for (char *c = buf; *c; ++c)
         if (*c == ' ') *c = '_';
     return buf;
@@ -184,7 +184,7 @@ cudaError_t plan_autotune(sbfs_handle *h, Plan &plan)
     // ---- classes 0 and 1: per-lane vs warp-pooled --------------------------
     for (int c = 0; c < 2; ++c) {
         const int n = kClassMaxN[c];
-        const int64_t count = 1 << 18;
+        const int64_t count = 1 << 20;   // the size of a typical large batch (the headline uses 1M)
         if ((e = prepare(b, n, count)) != cudaSuccess) break;
         Plan best = P;
         double best_ms = 1e30;

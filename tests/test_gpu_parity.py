@@ -187,3 +187,41 @@ def test_device_buffer_path(engine, oracle_mod):
     # the host path on the same handle afterwards still agrees
     host = engine.solve(recs, ns=ns)
     np.testing.assert_array_equal(host["len"], lens)
+
+
+def test_cuda_graph_replay_matches(oracle_mod):
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    recs = P.uniform_maps(120_000, 12, 901)
+    ns = P.uniform_sizes(50_000, 3, 18, 902)
+    mixed = P.uniform_maps(50_000, ns, 903)
+    ref = oracle_mod.solve(recs, n=12, words=False, threads=8)["len"]
+    ref_mixed = oracle_mod.solve(mixed, ns=ns, words=False, threads=8)["len"]
+    with sbfs.Engine(device=0, use_graph=True, chunk=1 << 16) as eng:
+        for rep in range(4):        # direct, captured, then replayed twice
+            r = eng.solve(recs, n=12)
+            np.testing.assert_array_equal(r["len"], ref)
+            assert oracle_mod.replay(recs, r["len"], r["words"], n=12)[0] == 0
+            m = eng.solve(mixed, ns=ns)
+            np.testing.assert_array_equal(m["len"], ref_mixed)
+        big = P.uniform_maps(300_000, 12, 904)   # larger chunks: buffers move, graphs rebuild
+        with sbfs.Engine(device=0, use_graph=True, chunk=1 << 18) as eng2:
+            for rep in range(3):
+                rb = eng2.solve(big, n=12)
+                rs = eng2.solve(recs, n=12)
+                np.testing.assert_array_equal(rs["len"], ref)
+        np.testing.assert_array_equal(rb["len"], oracle_mod.solve(big, n=12, words=False, threads=8)["len"])
+        dev = torch.device("cuda", 0)
+        d_maps = torch.from_numpy(recs).to(dev)
+        d_len = torch.empty(len(recs), dtype=torch.int32, device=dev)
+        d_words = torch.empty((len(recs), 2), dtype=torch.int64, device=dev)
+        d_fv = torch.empty(1, dtype=torch.int64, device=dev)
+        s = torch.cuda.Stream()
+        for rep in range(4):
+            d_len.fill_(-9)
+            torch.cuda.synchronize()
+            eng.solve_device(d_maps, 32, len(recs), n=12, d_len=d_len, d_words=d_words, word_stride=2,
+                             d_first_violation=d_fv, stream=s)
+            eng.wait_device()
+            np.testing.assert_array_equal(d_len.cpu().numpy(), ref)
