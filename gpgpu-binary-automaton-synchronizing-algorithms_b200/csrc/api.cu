@@ -338,8 +338,8 @@ sbfs_status ensure_plan(sbfs_handle *h)
     }
     const int lane_defaults[2][4] = {
         // warps, ring, refill_k
-        {4, 32, 16, 0},
-        {1, 32, 16, 0},
+        {8, 16, 16, 0},
+        {2, 32, 16, 0},
     };
     for (int c = 0; c < 2; ++c) {
         LaneShape &ls = P.lane[c];

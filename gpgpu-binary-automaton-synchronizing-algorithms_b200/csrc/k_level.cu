@@ -55,7 +55,9 @@ __global__ void __launch_bounds__(kThreads) k_level(LevelSlot *slots, uint64_t *
     const int lane = tid & 31;
     const int nslots = ctl->nslots;
     const unsigned long long total = ctl->total;
-    for (int i = tid; i <= nslots; i += blockDim.x) s_prefix[i] = ctl->prefix[i];
+    // slots admitted since the last transition (index >= prefix_n) have no work yet
+    const int pn = min(ctl->prefix_n, nslots);
+    for (int i = tid; i <= nslots; i += blockDim.x) s_prefix[i] = ctl->prefix[i <= pn ? i : pn];
 
     // ---- set-up of freshly admitted slots: clear bitmaps, build tables ------
     const size_t gtid = (size_t)blockIdx.x * blockDim.x + tid;
@@ -247,6 +249,7 @@ __global__ void __launch_bounds__(kThreads) k_level(LevelSlot *slots, uint64_t *
         unsigned long long total_new = 0;
         for (int q = 0; q < kThreads / 32; ++q) total_new += s_warp[q];
         ctl->total = total_new;
+        ctl->prefix_n = nslots;
         ctl->running = running;
         ctl->n_init = 0;
         ctl->launches += 1;

@@ -48,6 +48,8 @@ struct LevelCtl {
     unsigned int launches;
     unsigned long long total;    // items in the current levels of running slots
     unsigned long long expanded;
+    int prefix_n;                // slots the prefix below was computed for
+    int pad;
     unsigned long long prefix[kMaxLevelSlots + 1];
     int init_list[kMaxLevelSlots];
 };

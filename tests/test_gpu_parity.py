@@ -225,3 +225,19 @@ def test_cuda_graph_replay_matches(oracle_mod):
                              d_first_violation=d_fv, stream=s)
             eng.wait_device()
             np.testing.assert_array_equal(d_len.cpu().numpy(), ref)
+
+
+def test_level_slots_recycle_under_load(oracle_mod):
+    """More n=21 automata than level slots, with long (Cerny) and short ones
+    mixed, so slots finish, are freed and re-admitted while others run."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    recs = P.uniform_maps(600, 21, 1234)
+    for i in range(0, 600, 97):
+        recs[i] = P.cerny_record(21)
+    with sbfs.Engine(device=0) as eng:
+        r = eng.solve(recs, n=21)
+    ref = oracle_mod.solve(recs, n=21, words=False, threads=16)
+    np.testing.assert_array_equal(r["len"], ref["len"])
+    assert oracle_mod.replay(recs, r["len"], r["words"], n=21)[0] == 0
