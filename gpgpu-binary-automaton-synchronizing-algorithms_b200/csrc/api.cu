@@ -293,12 +293,13 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
     const bool lane_used = ((present & 1) && !P.use_pool[0]) || ((present & 2) && !P.use_pool[1]);
     if (!plain && lane_used) {
         // automata the per-lane kernel handed back (frontier wider than its ring,
-        // or a word longer than an entry carries) go through the pooled kernel
+        // or a word longer than an entry carries) are the heavy tail: the pooled
+        // kernel with a deep on-chip queue and small work grabs spreads them out
         Batch be = b;
         be.ns = j.ns;
         be.order = L.escal.as<int32_t>();
         be.range_dev = ctr->escal_range;
-        const PoolShape &s = P.pool[1];
+        const PoolShape &s = P.escal;
         CK(L.spill.reserve(pool_spill_words(s) * sizeof(uint32_t)), "allocating queue spill");
         CK(launch_pool(s, be, L.spill.as<uint32_t>(), &ctr->ticket[kNumClasses], st),
            "launching escalation kernel");
@@ -355,6 +356,14 @@ sbfs_status ensure_plan(sbfs_handle *h)
         if (per_sm < 1) return fail(h, SBFS_EINVAL, "per-lane kernel shape does not fit in shared memory");
         ls.ctas = per_sm * sms;
     }
+    P.escal = PoolShape{12, h->cfg.escal_slots > 0 ? h->cfg.escal_slots : 4, 2,
+                        h->cfg.escal_queue > 0 ? h->cfg.escal_queue : 256, 1,
+                        h->cfg.escal_grab > 0 ? h->cfg.escal_grab : 4};
+    {
+        const int per_sm = pool_max_ctas_per_sm(P.escal);
+        if (per_sm < 1) return fail(h, SBFS_EINVAL, "escalation kernel shape does not fit in shared memory");
+        P.escal.ctas = per_sm * sms;
+    }
     P.cta.threads = 512;
     P.cta.ctas = sms * 4;
     P.hbm.threads = 512;
@@ -404,6 +413,7 @@ sbfs_status reset_counters(sbfs_handle *h, Lane &L)
 struct Totals {
     int64_t first_violation = -1;
     int64_t expanded = 0;
+    int64_t escalated = 0;
     int error = 0;
     double kernel_ms = 0;
 };
@@ -416,6 +426,7 @@ sbfs_status finish_lane(sbfs_handle *h, Lane &L, Totals &t)
     const DevCounters *c = L.h_counters.as<DevCounters>();
     t.error |= c->error;
     t.expanded += (int64_t)c->expanded;
+    t.escalated += (int64_t)c->escal_range[1];
     if (c->first_violation != ULLONG_MAX) {
         const int64_t g = L.begin + (int64_t)c->first_violation;
         if (t.first_violation < 0 || g < t.first_violation) t.first_violation = g;
@@ -655,6 +666,7 @@ sbfs_status solve_host(sbfs_handle *h, const uint8_t *maps, int32_t lstride, con
         stats->launches = launches;
         stats->classes = 0;
         stats->kernel_ms = tot.kernel_ms;
+        stats->escalated = tot.escalated;
         stats->total_ms =
             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
@@ -897,6 +909,7 @@ sbfs_status sbfs_device_wait(sbfs_handle *h, sbfs_stats *stats)
         std::memset(stats, 0, sizeof(*stats));
         stats->automata = h->device_count;
         stats->expanded = (int64_t)c->expanded;
+        stats->escalated = (int64_t)c->escal_range[1];
         stats->launches = h->device_launches;
         float ms = 0;
         if (cudaEventElapsedTime(&ms, h->ev_dk0, h->ev_dk1) == cudaSuccess) stats->kernel_ms = ms;

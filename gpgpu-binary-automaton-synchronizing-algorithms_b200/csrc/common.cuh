@@ -84,6 +84,7 @@ struct PoolShape {
     int warps;         // warps per CTA
     int queue_smem;    // on-chip queue entries per automaton
     int ctas;          // grid size (persistent)
+    int grab = 16;     // automata a warp claims per work-ticket atomic
 };
 
 size_t pool_smem_bytes(const PoolShape &s);

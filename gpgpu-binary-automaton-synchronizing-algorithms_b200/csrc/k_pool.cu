@@ -26,8 +26,6 @@
 namespace sbfs {
 namespace {
 
-constexpr int kGrab = 16;   // automata claimed per ticket atomic
-
 template <int NMAX>
 struct PoolGeom {
     static constexpr int kBitmapWords = (1 << NMAX) / 32 > 0 ? (1 << NMAX) / 32 : 1;
@@ -55,7 +53,7 @@ __device__ __forceinline__ uint32_t table_image(const uint32_t *tb, uint32_t x)
 }
 
 template <int NMAX, int S>
-__global__ void __launch_bounds__(512) k_pool(Batch b, int q_smem, uint32_t *spill,
+__global__ void __launch_bounds__(512) k_pool(Batch b, int q_smem, int grab, uint32_t *spill,
                                               unsigned long long *ticket)
 {
     using G = PoolGeom<NMAX>;
@@ -108,10 +106,10 @@ __global__ void __launch_bounds__(512) k_pool(Batch b, int q_smem, uint32_t *spi
         while (free_mask && more) {
             if (cur == lim) {
                 unsigned long long got = 0;
-                if (lane == 0) got = atomicAdd(ticket, (unsigned long long)kGrab);
+                if (lane == 0) got = atomicAdd(ticket, (unsigned long long)grab);
                 got = __shfl_sync(kFull, got, 0);
                 cur = (int64_t)got;
-                lim = min((int64_t)got + kGrab, count);
+                lim = min((int64_t)got + grab, count);
                 if (cur >= count) {
                     more = false;
                     break;
@@ -326,7 +324,7 @@ cudaError_t launch_t(const PoolShape &s, const Batch &b, uint32_t *spill,
     cudaError_t e = cudaFuncSetAttribute(k_pool<NMAX, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    k_pool<NMAX, S><<<s.ctas, s.warps * 32, smem, st>>>(b, s.queue_smem, spill, ticket);
+    k_pool<NMAX, S><<<s.ctas, s.warps * 32, smem, st>>>(b, s.queue_smem, s.grab > 0 ? s.grab : 16, spill, ticket);
     return cudaGetLastError();
 }
 

@@ -111,6 +111,7 @@ struct Plan {
     CtaShape cta;
     CtaShape hbm;
     int use_pool[2];     // classes 0, 1: 1 = warp-pooled kernel instead of one automaton per lane
+    PoolShape escal;     // pooled kernel shape for automata the per-lane kernel handed back
     int class3_level;    // class 3: 1 = bitmaps in HBM (level slots) instead of shared memory (k_cta)
     int tuned;           // 1 when the autotuner (or its cache) chose the shapes
 };

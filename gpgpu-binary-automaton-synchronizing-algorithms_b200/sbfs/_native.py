@@ -53,6 +53,9 @@ class Config(ctypes.Structure):
         ("lane_refill", ctypes.c_int32),
         ("lane_warps", ctypes.c_int32),
         ("streams", ctypes.c_int32),
+        ("escal_slots", ctypes.c_int32),
+        ("escal_queue", ctypes.c_int32),
+        ("escal_grab", ctypes.c_int32),
         ("tune_cache", ctypes.c_char_p),
     ]
 
@@ -68,6 +71,7 @@ class Stats(ctypes.Structure):
         ("classes", ctypes.c_int32),
         ("kernel_ms", ctypes.c_double),
         ("total_ms", ctypes.c_double),
+        ("escalated", ctypes.c_int64),
     ]
 
     def as_dict(self):
