@@ -63,6 +63,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default kernel shapes")
     ap.add_argument("--no-graph", action="store_true", help="launch every step directly, no CUDA graphs")
+    ap.add_argument("--large-n", default="24,26,28", help="large workload: the state counts to include")
+    ap.add_argument("--level-arena-mb", type=int, default=0, help="HBM budget of the n > 20 level slots")
     return ap.parse_args()
 
 
@@ -70,7 +72,7 @@ def parse_args():
 # workloads
 # ---------------------------------------------------------------------------
 
-def make_workload(name: str, count: int, rank: int):
+def make_workload(name: str, count: int, rank: int, large_n=(24, 26, 28)):
     import numpy as np
     from sbfs import problem as P
 
@@ -95,7 +97,7 @@ def make_workload(name: str, count: int, rank: int):
                     desc=f"batched mixed: {count:,} automata, n uniform in 6..20, 1% Cerny family")
     if name == "large":
         rows, ns = [], []
-        for n in (24, 26, 28):
+        for n in large_n:
             r = P.uniform_maps(64, n, seed_base + 4 + n)
             rows.extend(list(r))
             ns.extend([n] * 64)
@@ -103,8 +105,9 @@ def make_workload(name: str, count: int, rank: int):
             rows.append(P.perm_merge_record(n, seed_base + 5 + n)); ns.append(n)
         recs = np.stack(rows)
         ns = np.array(ns, dtype=np.uint8)
-        return dict(recs=recs, ns=ns, n=0, lstride=32, max_n=28, count=len(ns),
-                    desc="large single instances: n=24,26,28 x (64 random + Cerny + permutation-plus-merge)")
+        return dict(recs=recs, ns=ns, n=0, lstride=32, max_n=max(large_n), count=len(ns),
+                    desc=f"large single instances: n={','.join(map(str, large_n))} x "
+                         "(64 random + Cerny + permutation-plus-merge)")
     raise ValueError(name)
 
 
@@ -187,7 +190,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    wl = make_workload(args.workload, args.count, 0)
+    wl = make_workload(args.workload, args.count, 0, tuple(int(x) for x in args.large_n.split(",")))
     threads = os.cpu_count() or 1
     import oracle
 
@@ -251,13 +254,13 @@ def run_sbfs(args):
     else:
         torch.cuda.set_device(0)
     dev = torch.device("cuda", torch.cuda.current_device())
-    wl = make_workload(args.workload, args.count, rank)
+    wl = make_workload(args.workload, args.count, rank, tuple(int(x) for x in args.large_n.split(",")))
     count, lstride = wl["count"], wl["lstride"]
     ws = sbfs.word_stride_for(wl["max_n"])
     import tempfile
     tune_cache = os.path.join(tempfile.gettempdir(), "sbfs_tune_cache.txt")
     eng = sbfs.Engine(device=dev.index, autotune=not args.no_tune, tune_cache=tune_cache,
-                      use_graph=not args.no_graph)
+                      use_graph=not args.no_graph, level_arena_bytes=args.level_arena_mb << 20)
     plan = eng.plan()   # runs the autotuner (or reads its cache) before any timing
 
     def barrier():

@@ -154,9 +154,9 @@ size_t level_arena_bytes(sbfs_handle *h, int max_n)
     size_t want = free_b / 2;
     const size_t cap = (size_t)64 << 30;
     if (want > cap) want = cap;
+    if (h->cfg.level_arena_bytes > 0) want = (size_t)h->cfg.level_arena_bytes;
     const size_t one = LevelEngine::footprint(max_n);
     if (want < one) want = one;   // at least one automaton of the largest size
-    (void)h;
     return want;
 }
 

@@ -56,6 +56,7 @@ class Config(ctypes.Structure):
         ("escal_slots", ctypes.c_int32),
         ("escal_queue", ctypes.c_int32),
         ("escal_grab", ctypes.c_int32),
+        ("level_arena_bytes", ctypes.c_int64),
         ("tune_cache", ctypes.c_char_p),
     ]
 

@@ -40,7 +40,7 @@ class Engine:
                  slots_per_warp: int = 0, warps_per_cta: int = 0, queue_smem: int = 0, chunk: int = 0,
                  small_kernel: int = 0, lane_ring: int = 0, lane_refill: int = 0, lane_warps: int = 0,
                  streams: int = 0, escal_slots: int = 0, escal_queue: int = 0, escal_grab: int = 0,
-                 tune_cache: Optional[str] = None):
+                 level_arena_bytes: int = 0, tune_cache: Optional[str] = None):
         self.lib = _native.load()
         cfg = _native.Config()
         self.lib.sbfs_config_default(ctypes.byref(cfg))
@@ -60,6 +60,7 @@ class Engine:
         cfg.escal_slots = escal_slots
         cfg.escal_queue = escal_queue
         cfg.escal_grab = escal_grab
+        cfg.level_arena_bytes = level_arena_bytes
         self._tune_cache = tune_cache.encode() if tune_cache else None
         cfg.tune_cache = self._tune_cache
         h = ctypes.c_void_p()

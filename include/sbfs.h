@@ -90,6 +90,7 @@ typedef struct sbfs_config {
     int32_t escal_slots;       /* heavy-tail pass: automata per warp; 0 = auto          */
     int32_t escal_queue;       /* heavy-tail pass: on-chip queue entries; 0 = auto      */
     int32_t escal_grab;        /* heavy-tail pass: automata per work ticket; 0 = auto   */
+    int64_t level_arena_bytes; /* HBM budget of the n > 20 level slots; 0 = half of free memory, <= 64 GiB */
     const char *tune_cache;    /* autotuner cache file, or NULL for in-memory only      */
 } sbfs_config;
 
