@@ -64,6 +64,8 @@ def parse_args():
     ap.add_argument("--no-tune", action="store_true", help="keep the default kernel shapes")
     ap.add_argument("--no-graph", action="store_true", help="launch every step directly, no CUDA graphs")
     ap.add_argument("--large-n", default="24,26,28", help="large workload: the state counts to include")
+    ap.add_argument("--large-kinds", default="random,cerny,perm",
+                    help="large workload: which families to include (random, cerny, perm)")
     ap.add_argument("--level-arena-mb", type=int, default=0, help="HBM budget of the n > 20 level slots")
     return ap.parse_args()
 
@@ -72,7 +74,7 @@ def parse_args():
 # workloads
 # ---------------------------------------------------------------------------
 
-def make_workload(name: str, count: int, rank: int, large_n=(24, 26, 28)):
+def make_workload(name: str, count: int, rank: int, large_n=(24, 26, 28), kinds=("random", "cerny", "perm")):
     import numpy as np
     from sbfs import problem as P
 
@@ -98,16 +100,19 @@ def make_workload(name: str, count: int, rank: int, large_n=(24, 26, 28)):
     if name == "large":
         rows, ns = [], []
         for n in large_n:
-            r = P.uniform_maps(64, n, seed_base + 4 + n)
-            rows.extend(list(r))
-            ns.extend([n] * 64)
-            rows.append(P.cerny_record(n)); ns.append(n)
-            rows.append(P.perm_merge_record(n, seed_base + 5 + n)); ns.append(n)
+            if "random" in kinds:
+                r = P.uniform_maps(64, n, seed_base + 4 + n)
+                rows.extend(list(r))
+                ns.extend([n] * 64)
+            if "cerny" in kinds:
+                rows.append(P.cerny_record(n)); ns.append(n)
+            if "perm" in kinds:
+                rows.append(P.perm_merge_record(n, seed_base + 5 + n)); ns.append(n)
         recs = np.stack(rows)
         ns = np.array(ns, dtype=np.uint8)
         return dict(recs=recs, ns=ns, n=0, lstride=32, max_n=max(large_n), count=len(ns),
                     desc=f"large single instances: n={','.join(map(str, large_n))} x "
-                         "(64 random + Cerny + permutation-plus-merge)")
+                         f"({' + '.join(kinds)})")
     raise ValueError(name)
 
 
@@ -190,7 +195,8 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    wl = make_workload(args.workload, args.count, 0, tuple(int(x) for x in args.large_n.split(",")))
+    wl = make_workload(args.workload, args.count, 0, tuple(int(x) for x in args.large_n.split(",")),
+                       tuple(args.large_kinds.split(",")))
     threads = os.cpu_count() or 1
     import oracle
 
@@ -254,7 +260,8 @@ def run_sbfs(args):
     else:
         torch.cuda.set_device(0)
     dev = torch.device("cuda", torch.cuda.current_device())
-    wl = make_workload(args.workload, args.count, rank, tuple(int(x) for x in args.large_n.split(",")))
+    wl = make_workload(args.workload, args.count, rank, tuple(int(x) for x in args.large_n.split(",")),
+                       tuple(args.large_kinds.split(",")))
     count, lstride = wl["count"], wl["lstride"]
     ws = sbfs.word_stride_for(wl["max_n"])
     import tempfile

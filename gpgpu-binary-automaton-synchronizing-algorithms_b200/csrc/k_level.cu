@@ -41,7 +41,7 @@ __device__ __forceinline__ int find_slot(const unsigned long long *prefix, int n
 }
 
 __global__ void __launch_bounds__(kThreads) k_level(LevelSlot *slots, uint64_t *tables, LevelCtl *ctl,
-                                                    Batch out)
+                                                    Batch out, int par)
 {
     __shared__ unsigned long long s_prefix[kMaxLevelSlots + 1];
     __shared__ uint64_t s_stage[kStage];
@@ -54,15 +54,22 @@ __global__ void __launch_bounds__(kThreads) k_level(LevelSlot *slots, uint64_t *
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int nslots = ctl->nslots;
-    const unsigned long long total = ctl->total;
+    const unsigned long long total = ctl->total[par];
+    // Only as many CTAs as the level needs take part (all of them while new
+    // slots are being set up); the others leave at once, so a small level
+    // does not pay for the whole grid's barriers and fences.
+    const int n_init = ctl->n_init[par];
+    const unsigned long long want = (total + blockDim.x - 1) / blockDim.x;
+    const int need = n_init > 0 ? (int)gridDim.x : (int)max(1ull, min((unsigned long long)gridDim.x, want));
+    if ((int)blockIdx.x >= need) return;
     // slots admitted since the last transition (index >= prefix_n) have no work yet
-    const int pn = min(ctl->prefix_n, nslots);
-    for (int i = tid; i <= nslots; i += blockDim.x) s_prefix[i] = ctl->prefix[i <= pn ? i : pn];
+    const int pn = min(ctl->prefix_n[par], nslots);
+    for (int i = tid; i <= nslots; i += blockDim.x) s_prefix[i] = ctl->prefix[par][i <= pn ? i : pn];
 
     // ---- set-up of freshly admitted slots: clear bitmaps, build tables ------
     const size_t gtid = (size_t)blockIdx.x * blockDim.x + tid;
-    const size_t gthreads = (size_t)gridDim.x * blockDim.x;
-    for (int q = 0; q < ctl->n_init; ++q) {
+    const size_t gthreads = (size_t)need * blockDim.x;
+    for (int q = 0; q < n_init; ++q) {
         const int s = ctl->init_list[q];
         LevelSlot &sl = slots[s];
         const size_t words4 = sl.n >= 7 ? ((size_t)1 << sl.n) / 128 : 1;
@@ -109,7 +116,9 @@ __global__ void __launch_bounds__(kThreads) k_level(LevelSlot *slots, uint64_t *
             for (int letter = 0; letter < 2; ++letter) {
                 const uint32_t y = letter ? (uint32_t)t : (uint32_t)(t >> 32);
                 const uint32_t m = 1u << (y & 31u);
-                if (!(atomicOr(sl.bitmap + (y >> 5), m) & m)) {
+                // bits only ever go 0 -> 1 during a search: a set bit seen by a
+                // plain load is final; otherwise the atomic decides who pushes
+                if (!(__ldcg(sl.bitmap + (y >> 5)) & m) && !(atomicOr(sl.bitmap + (y >> 5), m) & m)) {
                     if (is_singleton(y)) {
                         atomicMin(&sl.found, (idx << 1) | (unsigned long long)letter);
                     } else {
@@ -149,7 +158,7 @@ __global__ void __launch_bounds__(kThreads) k_level(LevelSlot *slots, uint64_t *
     // ---- the last CTA moves every slot to its next level ---------------------
     __threadfence();
     __syncthreads();
-    if (tid == 0) s_last = atomicAdd(&ctl->done_ctas, 1u) == gridDim.x - 1;
+    if (tid == 0) s_last = atomicAdd(&ctl->done_ctas, 1u) == (unsigned)need - 1;
     __syncthreads();
     if (!s_last) return;
     __threadfence();
@@ -243,15 +252,16 @@ __global__ void __launch_bounds__(kThreads) k_level(LevelSlot *slots, uint64_t *
     unsigned long long before = 0;
     for (int q = 0; q < (tid >> 5); ++q) before += s_warp[q];
     const unsigned long long excl = before + incl - w;
-    if (tid <= nslots) ctl->prefix[tid] = excl;   // prefix[nslots] = total (w = 0 there)
+    const int nxt = par ^ 1;
+    if (tid <= nslots) ctl->prefix[nxt][tid] = excl;   // prefix[nslots] = total (w = 0 there)
     const int running = __syncthreads_count(w > 0);
     if (tid == 0) {
         unsigned long long total_new = 0;
         for (int q = 0; q < kThreads / 32; ++q) total_new += s_warp[q];
-        ctl->total = total_new;
-        ctl->prefix_n = nslots;
+        ctl->total[nxt] = total_new;
+        ctl->prefix_n[nxt] = nslots;
         ctl->running = running;
-        ctl->n_init = 0;
+        ctl->n_init[nxt] = 0;
         ctl->launches += 1;
         ctl->done_ctas = 0;
         __threadfence();
@@ -270,11 +280,11 @@ int level_max_ctas_per_sm()
     return blocks;
 }
 
-cudaError_t launch_level(int ctas, LevelSlot *slots, uint64_t *tables, LevelCtl *ctl, const Batch &out,
+cudaError_t launch_level(int ctas, int parity, LevelSlot *slots, uint64_t *tables, LevelCtl *ctl, const Batch &out,
                          cudaStream_t st)
 {
     if (ctas < 1) return cudaErrorInvalidValue;
-    k_level<<<ctas, kThreads, 0, st>>>(slots, tables, ctl, out);
+    k_level<<<ctas, kThreads, 0, st>>>(slots, tables, ctl, out, parity & 1);
     return cudaGetLastError();
 }
 

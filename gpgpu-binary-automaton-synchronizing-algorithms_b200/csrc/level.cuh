@@ -39,23 +39,25 @@ struct LevelSlot {
     uint64_t word[kLevelWordU64];
 };
 
+// Control block.  Fields a launch reads at its start are double-buffered by
+// launch parity: launch t reads [t & 1] and its last CTA writes [(t+1) & 1],
+// so a CTA that starts late never sees the next level's values.
 struct LevelCtl {
     unsigned int done_ctas;
-    int nslots;                  // slot entries in use (highest index + 1)
-    int n_init;
+    int nslots;                  // slot entries in use (highest index + 1), host-written per launch batch
+    int n_init[2];               // freshly admitted slots to set up (host writes the batch's first parity)
     int running;
     unsigned int finished;       // slots that reached Done/Fail (monotone)
     unsigned int launches;
-    unsigned long long total;    // items in the current levels of running slots
+    int prefix_n[2];             // slots the prefix below was computed for
+    unsigned long long total[2]; // items in the current levels of running slots
     unsigned long long expanded;
-    int prefix_n;                // slots the prefix below was computed for
-    int pad;
-    unsigned long long prefix[kMaxLevelSlots + 1];
+    unsigned long long prefix[2][kMaxLevelSlots + 1];
     int init_list[kMaxLevelSlots];
 };
 
 int level_max_ctas_per_sm();
-cudaError_t launch_level(int ctas, LevelSlot *slots, uint64_t *tables, LevelCtl *ctl, const Batch &out,
+cudaError_t launch_level(int ctas, int parity, LevelSlot *slots, uint64_t *tables, LevelCtl *ctl, const Batch &out,
                          cudaStream_t st);
 
 // First-fit allocator over one device buffer (host-side bookkeeping only).
@@ -136,6 +138,7 @@ private:
     std::vector<int> pending_init_;
     int nslots_ = 0;
     int in_flight_ = 0;
+    unsigned long long parity_ = 0;   // launches issued so far (their parity selects the control buffers)
     bool launched_ = false;
     unsigned long long expanded_ = 0;
     int launches_ = 0;

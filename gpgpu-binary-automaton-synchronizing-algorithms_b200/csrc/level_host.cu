@@ -2,7 +2,6 @@
 // a first-fit arena for bitmaps and queues, admission into free slots, level
 // launches and collection of finished automata.
 #include <climits>
-#include <cstddef>
 #include <cstring>
 
 #include "level.cuh"
@@ -107,6 +106,7 @@ cudaError_t LevelEngine::init(int sm_count, size_t arena_bytes, cudaStream_t st)
     slot_off_.assign(kMaxLevelSlots, SIZE_MAX);
     nslots_ = 0;
     in_flight_ = 0;
+    parity_ = 0;
     return arena_.reserve(arena_bytes);
 }
 
@@ -175,21 +175,25 @@ cudaError_t LevelEngine::launch(int levels, const Batch &out)
             cudaSuccess)
             return e;
     }
-    // nslots, n_init and init_list are host-owned fields of the control block
-    static_assert(offsetof(LevelCtl, n_init) == offsetof(LevelCtl, nslots) + sizeof(int), "layout");
+    // nslots, this launch parity's n_init and init_list are host-owned
+    const int par = (int)(parity_ & 1);
     h_init_[0] = nslots_;
     h_init_[1] = (int)pending_init_.size();
     for (size_t i = 0; i < pending_init_.size(); ++i) h_init_[2 + i] = pending_init_[i];
     const int n_init = (int)pending_init_.size();
     pending_init_.clear();
-    if ((e = cudaMemcpyAsync(&d_ctl_->nslots, h_init_, sizeof(int) * 2, cudaMemcpyHostToDevice, st_)) !=
+    if ((e = cudaMemcpyAsync(&d_ctl_->nslots, h_init_, sizeof(int), cudaMemcpyHostToDevice, st_)) != cudaSuccess)
+        return e;
+    if ((e = cudaMemcpyAsync(&d_ctl_->n_init[par], h_init_ + 1, sizeof(int), cudaMemcpyHostToDevice, st_)) !=
         cudaSuccess)
         return e;
     if (n_init && (e = cudaMemcpyAsync(d_ctl_->init_list, h_init_ + 2, sizeof(int) * n_init,
                                        cudaMemcpyHostToDevice, st_)) != cudaSuccess)
         return e;
     for (int i = 0; i < levels; ++i) {
-        if ((e = launch_level(ctas_, d_slots_, d_tables_, d_ctl_, out, st_)) != cudaSuccess) return e;
+        if ((e = launch_level(ctas_, (int)(parity_ & 1), d_slots_, d_tables_, d_ctl_, out, st_)) != cudaSuccess)
+            return e;
+        ++parity_;
         ++launches_;
     }
     if ((e = cudaMemcpyAsync(h_slots_, d_slots_, sizeof(LevelSlot) * (size_t)nslots_, cudaMemcpyDeviceToHost,
