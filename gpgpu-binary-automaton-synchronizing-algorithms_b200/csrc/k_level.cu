@@ -46,6 +46,7 @@ __global__ void __launch_bounds__(kThreads) k_level(LevelSlot *slots, uint64_t *
     __shared__ unsigned long long s_prefix[kMaxLevelSlots + 1];
     __shared__ uint64_t s_stage[kStage];
     __shared__ unsigned short s_stage_slot[kStage];
+    __shared__ unsigned int s_stage_rank[kStage];
     __shared__ unsigned int s_count;
     __shared__ unsigned int s_slot_count[kMaxLevelSlots];
     __shared__ unsigned long long s_slot_base[kMaxLevelSlots];
@@ -95,60 +96,85 @@ __global__ void __launch_bounds__(kThreads) k_level(LevelSlot *slots, uint64_t *
     __syncthreads();
 
     // ---- one level of every running slot ------------------------------------
+    // Pushes are staged per CTA round; positions come from one shared atomic per
+    // warp (staging slot) and per warp and automaton (rank within the automaton),
+    // so no shared address is hammered by every thread.
     unsigned long long expanded = 0;
+    const unsigned lt = (1u << lane) - 1u;
     for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < total;
          base += gthreads) {
         if (tid == 0) s_count = 0;
         __syncthreads();
         const unsigned long long item = base + tid;
-        if (item < total) {
-            const int s = find_slot(s_prefix, nslots, item);
-            LevelSlot &sl = slots[s];
-            const unsigned long long idx = sl.lvl_start + (item - s_prefix[s]);
-            const uint32_t x = (uint32_t)(__ldcg(sl.queue + idx) & kLevelSubsetMask);
+        const bool have = item < total;
+        int s = 0;
+        unsigned long long idx = 0;
+        uint64_t t = 0;
+        LevelSlot *sl = nullptr;
+        if (have) {
+            s = find_slot(s_prefix, nslots, item);
+            sl = &slots[s];
+            idx = sl->lvl_start + (item - s_prefix[s]);
+            const uint32_t x = (uint32_t)(__ldcg(sl->queue + idx) & kLevelSubsetMask);
             const uint64_t *tb = tables + (size_t)s * kLevelTable;
-            uint64_t t = __ldg(tb + (x & 255u));
+            t = __ldg(tb + (x & 255u));
             t |= __ldg(tb + 256 + ((x >> 8) & 255u));
             t |= __ldg(tb + 512 + ((x >> 16) & 255u));
             t |= __ldg(tb + 768 + ((x >> 24) & 255u));
             ++expanded;
+        }
 #pragma unroll
-            for (int letter = 0; letter < 2; ++letter) {
-                const uint32_t y = letter ? (uint32_t)t : (uint32_t)(t >> 32);
+        for (int letter = 0; letter < 2; ++letter) {
+            const uint32_t y = letter ? (uint32_t)t : (uint32_t)(t >> 32);
+            bool push = false;
+            if (have) {
                 const uint32_t m = 1u << (y & 31u);
                 // bits only ever go 0 -> 1 during a search: a set bit seen by a
                 // plain load is final; otherwise the atomic decides who pushes
-                if (!(__ldcg(sl.bitmap + (y >> 5)) & m) && !(atomicOr(sl.bitmap + (y >> 5), m) & m)) {
-                    if (is_singleton(y)) {
-                        atomicMin(&sl.found, (idx << 1) | (unsigned long long)letter);
-                    } else {
-                        const unsigned int pos = atomicAdd(&s_count, 1u);
-                        s_stage[pos] = (uint64_t)y | (idx << 28) | ((uint64_t)letter << 63);
-                        s_stage_slot[pos] = (unsigned short)s;
-                        atomicAdd(&s_slot_count[s], 1u);
-                    }
+                if (!(__ldcg(sl->bitmap + (y >> 5)) & m) && !(atomicOr(sl->bitmap + (y >> 5), m) & m)) {
+                    if (is_singleton(y))
+                        atomicMin(&sl->found, (idx << 1) | (unsigned long long)letter);
+                    else
+                        push = true;
+                }
+            }
+            const unsigned pm = __ballot_sync(kFull, push);
+            if (pm) {
+                unsigned int pos = 0;
+                const int leader = __ffs(pm) - 1;
+                if (lane == leader) pos = atomicAdd(&s_count, (unsigned)__popc(pm));
+                pos = __shfl_sync(kFull, pos, leader) + __popc(pm & lt);
+                if (push) {
+                    const unsigned grp = __match_any_sync(pm, s);
+                    const int gl = __ffs(grp) - 1;
+                    unsigned int r0 = 0;
+                    if (lane == gl) r0 = atomicAdd(&s_slot_count[s], (unsigned)__popc(grp));
+                    const unsigned int rank = __shfl_sync(grp, r0, gl) + __popc(grp & lt);
+                    s_stage[pos] = (uint64_t)y | (idx << 28) | ((uint64_t)letter << 63);
+                    s_stage_slot[pos] = (unsigned short)s;
+                    s_stage_rank[pos] = rank;
                 }
             }
         }
         __syncthreads();
         // reserve space per slot: one global atomic per slot with pushes this round
-        for (int s = tid; s < nslots; s += blockDim.x) {
-            const unsigned int c = s_slot_count[s];
+        for (int q = tid; q < nslots; q += blockDim.x) {
+            const unsigned int c = s_slot_count[q];
             if (c) {
-                s_slot_base[s] = atomicAdd(&slots[s].tail, (unsigned long long)c);
-                s_slot_count[s] = 0;
+                s_slot_base[q] = atomicAdd(&slots[q].tail, (unsigned long long)c);
+                s_slot_count[q] = 0;
             }
         }
         __syncthreads();
         const unsigned int cnt = s_count;
         for (unsigned int p = tid; p < cnt; p += blockDim.x) {
-            const int s = s_stage_slot[p];
-            const unsigned long long pos = atomicAdd(&s_slot_base[s], 1ull);
-            LevelSlot &sl = slots[s];
-            if (pos < sl.cap)
-                __stcg(sl.queue + pos, s_stage[p]);
+            const int q = s_stage_slot[p];
+            const unsigned long long pos = s_slot_base[q] + s_stage_rank[p];
+            LevelSlot &dst = slots[q];
+            if (pos < dst.cap)
+                __stcg(dst.queue + pos, s_stage[p]);
             else
-                atomicOr(&sl.overflow, 1);
+                atomicOr(&dst.overflow, 1);
         }
         __syncthreads();
     }
