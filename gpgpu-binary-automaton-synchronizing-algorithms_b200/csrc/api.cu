@@ -209,7 +209,7 @@ sbfs_status run_level_class(sbfs_handle *h, Lane &L, const Job &j, const Batch &
             ++next;
         }
         if (E.in_flight() == 0) return fail(h, SBFS_ENOMEM, "level-slot arena cannot hold one automaton");
-        CK(E.launch(levels, bc), "launching level kernels");
+        CK(E.launch(levels, bc, 4096), "launching level kernels");
         *launches += levels;
         done.clear();
         CK(E.collect(done), "collecting level slots");

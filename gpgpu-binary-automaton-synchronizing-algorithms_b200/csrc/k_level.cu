@@ -26,6 +26,19 @@ namespace {
 constexpr int kThreads = 512;
 constexpr int kStage = 2 * kThreads;   // staged pushes per CTA round
 
+struct LevelSmem {
+    unsigned long long prefix[kMaxLevelSlots + 1];
+    uint64_t stage[kStage];
+    unsigned short stage_slot[kStage];
+    unsigned int stage_rank[kStage];
+    unsigned int count;
+    unsigned int slot_count[kMaxLevelSlots];
+    unsigned long long slot_base[kMaxLevelSlots];
+    unsigned long long warp_sum[kThreads / 32];
+    bool last;
+};
+
+
 __device__ __forceinline__ int find_slot(const unsigned long long *prefix, int nslots, unsigned long long item)
 {
     // largest s with prefix[s] <= item (prefix[0] = 0, nondecreasing)
@@ -40,70 +53,23 @@ __device__ __forceinline__ int find_slot(const unsigned long long *prefix, int n
     return lo;
 }
 
-__global__ void __launch_bounds__(kThreads) k_level(LevelSlot *slots, uint64_t *tables, LevelCtl *ctl,
-                                                    Batch out, int par)
+// Expands this CTA's share of the current level of every running slot: items
+// [cta * blockDim, ...) with stride ncta * blockDim over the concatenation of
+// the slots' levels (sh.prefix).  Returns the number of subsets expanded.
+__device__ unsigned long long level_items(LevelSlot *slots, const uint64_t *tables, LevelSmem &sh, int nslots,
+                                          unsigned long long total, int cta, int ncta)
 {
-    __shared__ unsigned long long s_prefix[kMaxLevelSlots + 1];
-    __shared__ uint64_t s_stage[kStage];
-    __shared__ unsigned short s_stage_slot[kStage];
-    __shared__ unsigned int s_stage_rank[kStage];
-    __shared__ unsigned int s_count;
-    __shared__ unsigned int s_slot_count[kMaxLevelSlots];
-    __shared__ unsigned long long s_slot_base[kMaxLevelSlots];
-    __shared__ bool s_last;
-
     const int tid = threadIdx.x;
     const int lane = tid & 31;
-    const int nslots = ctl->nslots;
-    const unsigned long long total = ctl->total[par];
-    // Only as many CTAs as the level needs take part (all of them while new
-    // slots are being set up); the others leave at once, so a small level
-    // does not pay for the whole grid's barriers and fences.
-    const int n_init = ctl->n_init[par];
-    const unsigned long long want = (total + blockDim.x - 1) / blockDim.x;
-    const int need = n_init > 0 ? (int)gridDim.x : (int)max(1ull, min((unsigned long long)gridDim.x, want));
-    if ((int)blockIdx.x >= need) return;
-    // slots admitted since the last transition (index >= prefix_n) have no work yet
-    const int pn = min(ctl->prefix_n[par], nslots);
-    for (int i = tid; i <= nslots; i += blockDim.x) s_prefix[i] = ctl->prefix[par][i <= pn ? i : pn];
-
-    // ---- set-up of freshly admitted slots: clear bitmaps, build tables ------
-    const size_t gtid = (size_t)blockIdx.x * blockDim.x + tid;
-    const size_t gthreads = (size_t)need * blockDim.x;
-    for (int q = 0; q < n_init; ++q) {
-        const int s = ctl->init_list[q];
-        LevelSlot &sl = slots[s];
-        const size_t words4 = sl.n >= 7 ? ((size_t)1 << sl.n) / 128 : 1;
-        uint4 *bm4 = reinterpret_cast<uint4 *>(sl.bitmap);
-        for (size_t w = gtid; w < words4; w += gthreads) bm4[w] = make_uint4(0u, 0u, 0u, 0u);
-        uint64_t *tb = tables + (size_t)s * kLevelTable;
-        for (size_t e = gtid; e < kLevelTable; e += gthreads) {
-            const int c = (int)(e >> 8), v = (int)(e & 255);
-            uint32_t ta = 0, tbv = 0;
-            for (int j = 0; j < 8; ++j) {
-                const int st = 8 * c + j;
-                if (((v >> j) & 1) && st < sl.n) {
-                    const uint32_t av = sl.rec ? sl.rec[st] : sl.a[st];
-                    const uint32_t bv = sl.rec ? sl.rec[sl.lstride + st] : sl.b[st];
-                    ta |= 1u << (av & 31u);
-                    tbv |= 1u << (bv & 31u);
-                }
-            }
-            tb[e] = ((uint64_t)ta << 32) | tbv;
-        }
-    }
-    if (tid < kMaxLevelSlots) s_slot_count[tid] = 0;
-    __syncthreads();
-
+    const unsigned long long gthreads = (unsigned long long)ncta * blockDim.x;
     // ---- one level of every running slot ------------------------------------
     // Pushes are staged per CTA round; positions come from one shared atomic per
     // warp (staging slot) and per warp and automaton (rank within the automaton),
     // so no shared address is hammered by every thread.
     unsigned long long expanded = 0;
     const unsigned lt = (1u << lane) - 1u;
-    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < total;
-         base += gthreads) {
-        if (tid == 0) s_count = 0;
+    for (unsigned long long base = (unsigned long long)cta * blockDim.x; base < total; base += gthreads) {
+        if (tid == 0) sh.count = 0;
         __syncthreads();
         const unsigned long long item = base + tid;
         const bool have = item < total;
@@ -112,9 +78,9 @@ __global__ void __launch_bounds__(kThreads) k_level(LevelSlot *slots, uint64_t *
         uint64_t t = 0;
         LevelSlot *sl = nullptr;
         if (have) {
-            s = find_slot(s_prefix, nslots, item);
+            s = find_slot(sh.prefix, nslots, item);
             sl = &slots[s];
-            idx = sl->lvl_start + (item - s_prefix[s]);
+            idx = sl->lvl_start + (item - sh.prefix[s]);
             const uint32_t x = (uint32_t)(__ldcg(sl->queue + idx) & kLevelSubsetMask);
             const uint64_t *tb = tables + (size_t)s * kLevelTable;
             t = __ldg(tb + (x & 255u));
@@ -142,52 +108,55 @@ __global__ void __launch_bounds__(kThreads) k_level(LevelSlot *slots, uint64_t *
             if (pm) {
                 unsigned int pos = 0;
                 const int leader = __ffs(pm) - 1;
-                if (lane == leader) pos = atomicAdd(&s_count, (unsigned)__popc(pm));
+                if (lane == leader) pos = atomicAdd(&sh.count, (unsigned)__popc(pm));
                 pos = __shfl_sync(kFull, pos, leader) + __popc(pm & lt);
                 if (push) {
                     const unsigned grp = __match_any_sync(pm, s);
                     const int gl = __ffs(grp) - 1;
                     unsigned int r0 = 0;
-                    if (lane == gl) r0 = atomicAdd(&s_slot_count[s], (unsigned)__popc(grp));
+                    if (lane == gl) r0 = atomicAdd(&sh.slot_count[s], (unsigned)__popc(grp));
                     const unsigned int rank = __shfl_sync(grp, r0, gl) + __popc(grp & lt);
-                    s_stage[pos] = (uint64_t)y | (idx << 28) | ((uint64_t)letter << 63);
-                    s_stage_slot[pos] = (unsigned short)s;
-                    s_stage_rank[pos] = rank;
+                    sh.stage[pos] = (uint64_t)y | (idx << 28) | ((uint64_t)letter << 63);
+                    sh.stage_slot[pos] = (unsigned short)s;
+                    sh.stage_rank[pos] = rank;
                 }
             }
         }
         __syncthreads();
         // reserve space per slot: one global atomic per slot with pushes this round
         for (int q = tid; q < nslots; q += blockDim.x) {
-            const unsigned int c = s_slot_count[q];
+            const unsigned int c = sh.slot_count[q];
             if (c) {
-                s_slot_base[q] = atomicAdd(&slots[q].tail, (unsigned long long)c);
-                s_slot_count[q] = 0;
+                sh.slot_base[q] = atomicAdd(&slots[q].tail, (unsigned long long)c);
+                sh.slot_count[q] = 0;
             }
         }
         __syncthreads();
-        const unsigned int cnt = s_count;
+        const unsigned int cnt = sh.count;
         for (unsigned int p = tid; p < cnt; p += blockDim.x) {
-            const int q = s_stage_slot[p];
-            const unsigned long long pos = s_slot_base[q] + s_stage_rank[p];
+            const int q = sh.stage_slot[p];
+            const unsigned long long pos = sh.slot_base[q] + sh.stage_rank[p];
             LevelSlot &dst = slots[q];
             if (pos < dst.cap)
-                __stcg(dst.queue + pos, s_stage[p]);
+                __stcg(dst.queue + pos, sh.stage[p]);
             else
                 atomicOr(&dst.overflow, 1);
         }
         __syncthreads();
     }
-    for (int o = 16; o; o >>= 1) expanded += __shfl_down_sync(kFull, expanded, o);
-    if (lane == 0 && expanded) atomicAdd(&ctl->expanded, expanded);
+    return expanded;
+}
 
-    // ---- the last CTA moves every slot to its next level ---------------------
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) s_last = atomicAdd(&ctl->done_ctas, 1u) == (unsigned)need - 1;
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
+// Moves every slot to its next level (all threads of one CTA): finishes the
+// slots that found a singleton or ran dry (word by parent pointers), turns
+// freshly admitted slots into running ones, and writes the prefix sums of the
+// new levels to prefix_out.  Returns the new total (block-uniform); `running`
+// receives the number of running slots.
+__device__ unsigned long long level_transition(LevelSlot *slots, LevelCtl *ctl, const Batch &out, LevelSmem &sh,
+                                               int nslots, unsigned long long *prefix_out, int &running)
+{
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
     for (int s = tid; s < nslots; s += blockDim.x) {
         LevelSlot &sl = slots[s];
         const int st = *(volatile int *)&sl.state;
@@ -260,36 +229,135 @@ __global__ void __launch_bounds__(kThreads) k_level(LevelSlot *slots, uint64_t *
             }
         }
     }
-    // prefix sums of the new levels (block-wide scan over the slots)
-    __shared__ unsigned long long s_width[kMaxLevelSlots];
-    __shared__ unsigned long long s_warp[kThreads / 32];
     __syncthreads();
     unsigned long long w = 0;
     if (tid < nslots && slots[tid].state == kSlotRun) w = slots[tid].lvl_end - slots[tid].lvl_start;
-    if (tid < kMaxLevelSlots) s_width[tid] = w;
     unsigned long long incl = w;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
         const unsigned long long y = __shfl_up_sync(kFull, incl, d);
         if (lane >= d) incl += y;
     }
-    if (lane == 31) s_warp[tid >> 5] = incl;
+    if (lane == 31) sh.warp_sum[tid >> 5] = incl;
     __syncthreads();
     unsigned long long before = 0;
-    for (int q = 0; q < (tid >> 5); ++q) before += s_warp[q];
+    for (int q = 0; q < (tid >> 5); ++q) before += sh.warp_sum[q];
     const unsigned long long excl = before + incl - w;
+    running = __syncthreads_count(w > 0);
+    if (tid <= nslots) prefix_out[tid] = excl;   // prefix_out[nslots] = total (w = 0 there)
+    unsigned long long total_new = 0;
+    for (int q = 0; q < kThreads / 32; ++q) total_new += sh.warp_sum[q];
+    __syncthreads();
+    return total_new;
+}
+
+__global__ void __launch_bounds__(kThreads) k_level(LevelSlot *slots, uint64_t *tables, LevelCtl *ctl,
+                                                    Batch out, int par)
+{
+    __shared__ LevelSmem sh;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int nslots = ctl->nslots;
+    const unsigned long long total = ctl->total[par];
+    // Only as many CTAs as the level needs take part (all of them while new
+    // slots are being set up); the others leave at once, so a small level
+    // does not pay for the whole grid's barriers and fences.
+    const int n_init = ctl->n_init[par];
+    const unsigned long long want = (total + blockDim.x - 1) / blockDim.x;
+    const int need = n_init > 0 ? (int)gridDim.x : (int)max(1ull, min((unsigned long long)gridDim.x, want));
+    if ((int)blockIdx.x >= need) return;
+    // slots admitted since the last transition (index >= prefix_n) have no work yet
+    const int pn = min(ctl->prefix_n[par], nslots);
+    for (int i = tid; i <= nslots; i += blockDim.x) sh.prefix[i] = ctl->prefix[par][i <= pn ? i : pn];
+
+    // ---- set-up of freshly admitted slots: clear bitmaps, build tables ------
+    const size_t gtid = (size_t)blockIdx.x * blockDim.x + tid;
+    const size_t gthreads = (size_t)need * blockDim.x;
+    for (int q = 0; q < n_init; ++q) {
+        const int s = ctl->init_list[q];
+        LevelSlot &sl = slots[s];
+        const size_t words4 = sl.n >= 7 ? ((size_t)1 << sl.n) / 128 : 1;
+        uint4 *bm4 = reinterpret_cast<uint4 *>(sl.bitmap);
+        for (size_t w = gtid; w < words4; w += gthreads) bm4[w] = make_uint4(0u, 0u, 0u, 0u);
+        uint64_t *tb = tables + (size_t)s * kLevelTable;
+        for (size_t e = gtid; e < kLevelTable; e += gthreads) {
+            const int c = (int)(e >> 8), v = (int)(e & 255);
+            uint32_t ta = 0, tbv = 0;
+            for (int j = 0; j < 8; ++j) {
+                const int st = 8 * c + j;
+                if (((v >> j) & 1) && st < sl.n) {
+                    const uint32_t av = sl.rec ? sl.rec[st] : sl.a[st];
+                    const uint32_t bv = sl.rec ? sl.rec[sl.lstride + st] : sl.b[st];
+                    ta |= 1u << (av & 31u);
+                    tbv |= 1u << (bv & 31u);
+                }
+            }
+            tb[e] = ((uint64_t)ta << 32) | tbv;
+        }
+    }
+    if (tid < kMaxLevelSlots) sh.slot_count[tid] = 0;
+    __syncthreads();
+
+    unsigned long long expanded = level_items(slots, tables, sh, nslots, total, blockIdx.x, need);
+    for (int o = 16; o; o >>= 1) expanded += __shfl_down_sync(kFull, expanded, o);
+    if (lane == 0 && expanded) atomicAdd(&ctl->expanded, expanded);
+
+    // ---- the last CTA moves every slot to its next level ---------------------
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) sh.last = atomicAdd(&ctl->done_ctas, 1u) == (unsigned)need - 1;
+    __syncthreads();
+    if (!sh.last) return;
+    __threadfence();
     const int nxt = par ^ 1;
-    if (tid <= nslots) ctl->prefix[nxt][tid] = excl;   // prefix[nslots] = total (w = 0 there)
-    const int running = __syncthreads_count(w > 0);
+    int running = 0;
+    const unsigned long long total_new = level_transition(slots, ctl, out, sh, nslots, ctl->prefix[nxt], running);
     if (tid == 0) {
-        unsigned long long total_new = 0;
-        for (int q = 0; q < kThreads / 32; ++q) total_new += s_warp[q];
         ctl->total[nxt] = total_new;
         ctl->prefix_n[nxt] = nslots;
         ctl->running = running;
         ctl->n_init[nxt] = 0;
         ctl->launches += 1;
         ctl->done_ctas = 0;
+        __threadfence();
+    }
+}
+
+// Narrow levels: one CTA runs consecutive levels by itself -- expand, move to
+// the next level, repeat -- while the levels stay at most `narrow` subsets
+// wide, up to `max_levels` levels, with no launch or grid barrier in between.
+// It is launched as a grid of one CTA, and only when no slot awaits set-up.
+__global__ void __launch_bounds__(kThreads) k_level_narrow(LevelSlot *slots, uint64_t *tables, LevelCtl *ctl,
+                                                           Batch out, int par, int max_levels,
+                                                           unsigned long long narrow)
+{
+    __shared__ LevelSmem sh;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int nslots = ctl->nslots;
+    unsigned long long total = ctl->total[par];
+    const int pn = min(ctl->prefix_n[par], nslots);
+    for (int i = tid; i <= nslots; i += blockDim.x) sh.prefix[i] = ctl->prefix[par][i <= pn ? i : pn];
+    if (tid < kMaxLevelSlots) sh.slot_count[tid] = 0;
+    __syncthreads();
+    unsigned long long expanded = 0;
+    int running = 0;
+    for (int it = 0; it < max_levels; ++it) {
+        expanded += level_items(slots, tables, sh, nslots, total, 0, 1);
+        __syncthreads();
+        total = level_transition(slots, ctl, out, sh, nslots, sh.prefix, running);
+        if (running == 0 || total > narrow) break;
+    }
+    for (int o = 16; o; o >>= 1) expanded += __shfl_down_sync(kFull, expanded, o);
+    if (lane == 0 && expanded) atomicAdd(&ctl->expanded, expanded);
+    const int nxt = par ^ 1;
+    for (int i = tid; i <= nslots; i += blockDim.x) ctl->prefix[nxt][i] = sh.prefix[i];
+    if (tid == 0) {
+        ctl->total[nxt] = total;
+        ctl->prefix_n[nxt] = nslots;
+        ctl->running = running;
+        ctl->n_init[nxt] = 0;
+        ctl->launches += 1;
         __threadfence();
     }
 }
@@ -311,6 +379,14 @@ cudaError_t launch_level(int ctas, int parity, LevelSlot *slots, uint64_t *table
 {
     if (ctas < 1) return cudaErrorInvalidValue;
     k_level<<<ctas, kThreads, 0, st>>>(slots, tables, ctl, out, parity & 1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_level_narrow(int parity, int max_levels, unsigned long long narrow, LevelSlot *slots,
+                                uint64_t *tables, LevelCtl *ctl, const Batch &out, cudaStream_t st)
+{
+    if (max_levels < 1) return cudaErrorInvalidValue;
+    k_level_narrow<<<1, kThreads, 0, st>>>(slots, tables, ctl, out, parity & 1, max_levels, narrow);
     return cudaGetLastError();
 }
 

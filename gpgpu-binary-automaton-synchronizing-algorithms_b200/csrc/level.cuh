@@ -59,6 +59,11 @@ struct LevelCtl {
 int level_max_ctas_per_sm();
 cudaError_t launch_level(int ctas, int parity, LevelSlot *slots, uint64_t *tables, LevelCtl *ctl, const Batch &out,
                          cudaStream_t st);
+cudaError_t launch_level_narrow(int parity, int max_levels, unsigned long long narrow, LevelSlot *slots,
+                                uint64_t *tables, LevelCtl *ctl, const Batch &out, cudaStream_t st);
+
+// Level totals at or below this are expanded by one CTA looping over levels.
+constexpr unsigned long long kNarrowLevel = 4096;
 
 // First-fit allocator over one device buffer (host-side bookkeeping only).
 class Arena {
@@ -91,9 +96,11 @@ public:
     // admit one automaton whose record is at d_rec (device); returns slot or -1 (no slot/memory)
     int admit(const uint8_t *d_rec, int lstride, int n, long long tag, const uint8_t *host_a,
               const uint8_t *host_b);
-    // upload admissions, launch `levels` level kernels, copy slot states back (async);
-    // results go to `out` when out.out_len is set (batch mode)
-    cudaError_t launch(int levels, const Batch &out);
+    // upload admissions, launch `levels` level kernels -- or, when the current
+    // levels are narrow and nothing awaits set-up, one single-CTA launch that
+    // runs up to `narrow_levels` narrow levels -- then copy slot states back
+    // (async); results go to `out` when out.out_len is set (batch mode)
+    cudaError_t launch(int levels, const Batch &out, int narrow_levels = 0);
     // wait for the last launch and collect finished slots (frees their memory)
     struct Finished {
         long long tag;

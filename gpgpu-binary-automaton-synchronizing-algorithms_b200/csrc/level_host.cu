@@ -166,9 +166,12 @@ int LevelEngine::admit(const uint8_t *d_rec, int lstride, int n, long long tag, 
     return s;
 }
 
-cudaError_t LevelEngine::launch(int levels, const Batch &out)
+cudaError_t LevelEngine::launch(int levels, const Batch &out, int narrow_levels)
 {
     cudaError_t e;
+    // the last copied control block holds the totals the next launch will read
+    const bool narrow = narrow_levels > 0 && pending_init_.empty() && launches_ > 0 &&
+                        h_ctl_->total[parity_ & 1] <= kNarrowLevel;
     // admissions: descriptors of the new slots, then the control block's init list
     for (int s : pending_init_) {
         if ((e = cudaMemcpyAsync(d_slots_ + s, h_slots_ + s, sizeof(LevelSlot), cudaMemcpyHostToDevice, st_)) !=
@@ -190,11 +193,19 @@ cudaError_t LevelEngine::launch(int levels, const Batch &out)
     if (n_init && (e = cudaMemcpyAsync(d_ctl_->init_list, h_init_ + 2, sizeof(int) * n_init,
                                        cudaMemcpyHostToDevice, st_)) != cudaSuccess)
         return e;
-    for (int i = 0; i < levels; ++i) {
-        if ((e = launch_level(ctas_, (int)(parity_ & 1), d_slots_, d_tables_, d_ctl_, out, st_)) != cudaSuccess)
+    if (narrow) {
+        if ((e = launch_level_narrow((int)(parity_ & 1), narrow_levels, kNarrowLevel, d_slots_, d_tables_, d_ctl_, out,
+                                     st_)) != cudaSuccess)
             return e;
         ++parity_;
         ++launches_;
+    } else {
+        for (int i = 0; i < levels; ++i) {
+            if ((e = launch_level(ctas_, (int)(parity_ & 1), d_slots_, d_tables_, d_ctl_, out, st_)) != cudaSuccess)
+                return e;
+            ++parity_;
+            ++launches_;
+        }
     }
     if ((e = cudaMemcpyAsync(h_slots_, d_slots_, sizeof(LevelSlot) * (size_t)nslots_, cudaMemcpyDeviceToHost,
                              st_)) != cudaSuccess)

@@ -213,7 +213,7 @@ void run_loop(sbfs_server *s)
                 s->pend_large.pop_front();
             }
             if (s->level.in_flight() > 0) {
-                s->level.launch(s->cfg.max_levels, none);
+                s->level.launch(s->cfg.max_levels, none, 4 * s->cfg.max_levels);
                 std::lock_guard<std::mutex> lock(s->mu);
                 s->st.level_launches += s->cfg.max_levels;
                 progress = true;
