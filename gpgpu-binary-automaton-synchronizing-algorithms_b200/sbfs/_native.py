@@ -21,6 +21,7 @@ EXPORTS = [
     "sbfs_host_free", "sbfs_word_stride", "sbfs_describe_plan", "sbfs_solve_small_noalloc",
     "sbfs_server_config_default", "sbfs_server_start", "sbfs_server_submit", "sbfs_server_poll",
     "sbfs_server_cancel", "sbfs_server_stats_get", "sbfs_server_reset_peak", "sbfs_server_stop",
+    "sbfs_generate_reference_batch", "sbfs_dotnet_random_next",
 ]
 
 STATUS = {0: "SBFS_OK", 1: "SBFS_EINVAL", 2: "SBFS_ENOMEM", 3: "SBFS_ETIMEOUT", 4: "SBFS_ECUDA",
@@ -176,6 +177,10 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.sbfs_describe_plan.restype = i32
     L.sbfs_host_free.argtypes = [P]
     L.sbfs_host_free.restype = ctypes.c_int
+    L.sbfs_generate_reference_batch.argtypes = [i64, i32, i32, P, i32]
+    L.sbfs_generate_reference_batch.restype = ctypes.c_int
+    L.sbfs_dotnet_random_next.argtypes = [i32, i32, P]
+    L.sbfs_dotnet_random_next.restype = ctypes.c_int
     _lib = L
     return L
 

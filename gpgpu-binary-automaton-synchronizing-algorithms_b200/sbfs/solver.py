@@ -225,3 +225,30 @@ class SlimGPUNative:
                degreeOfParallelism: int) -> int:  # IComputable.cs:17
         return self.Compute(problemsToSolve, problemsReadingIndex, None, -1, problemCount,
                             degreeOfParallelism)
+
+
+CERNY_FAILED_CSV = "./cernyFailed.csv"
+
+
+def verify_and_report(solver, problems: Sequence[Problem], path: str = CERNY_FAILED_CSV) -> int:
+    """The benchmark's Verify step (GPGPU/Program.cs:108-129): run
+    ``solver.Verify`` over all ``problems`` at its best parallelism; when an
+    automaton's shortest word is longer than (n-1)^2, append that automaton's
+    ``ToString()`` to ``path`` (``File.AppendAllText``: no separator, as the
+    reference writes it) and return its index, else return -1."""
+    result = solver.Verify(problems, 0, len(problems), solver.GetBestParallelism())
+    if result >= 0:
+        with open(path, "a", encoding="utf-8") as f:
+            f.write(str(problems[result]))
+    return result
+
+
+def read_cerny_failed(path: str = CERNY_FAILED_CSV) -> List[Problem]:
+    """Automata appended by :func:`verify_and_report` (or by the reference),
+    split at the ``]][[`` joints the separator-less appends leave."""
+    with open(path, encoding="utf-8") as f:
+        text = f.read().strip()
+    if not text:
+        return []
+    parts = text.replace("]][[", "]]\n[[").split("\n")
+    return [Problem.parse(p) for p in parts if p.strip()]

@@ -255,6 +255,21 @@ SBFS_API sbfs_status sbfs_server_stop(sbfs_server *s);
  * ceil((max_n-1)^2 / 64), at least 1. */
 SBFS_API int32_t sbfs_word_stride(int32_t max_n);
 
+/* ---------------------------------------------------------------------------
+ * The reference's input batches, bit for bit (host code, no GPU).  The
+ * reference draws automata with .NET Framework's System.Random (Knuth's
+ * subtractive generator): Problem.FillArrayOfProblems(problems, count, n, seed)
+ * (SharedDefinitions/Problem.cs:32-58) seeds Random(seed) and builds each
+ * automaton from Random(master.Next()), A[i] then B[i] = Next(0, n).  GPGPU's
+ * benchmark uses seed 1234567 + count (GPGPU/Program.cs:94).
+ * ------------------------------------------------------------------------- */
+/* count records of 2*lstride bytes (a = rec[0..n), b = rec[lstride..lstride+n),
+ * bytes past n zero); 1 <= n <= lstride <= 32. */
+SBFS_API sbfs_status sbfs_generate_reference_batch(int64_t count, int32_t n, int32_t seed, uint8_t *maps,
+                                                   int32_t lstride);
+/* The first count values of new System.Random(seed).Next(). */
+SBFS_API sbfs_status sbfs_dotnet_random_next(int32_t seed, int32_t count, int32_t *out);
+
 #ifdef __cplusplus
 }
 #endif

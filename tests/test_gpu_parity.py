@@ -44,6 +44,29 @@ def test_config2_n12_full_batch_and_sample(engine, oracle_mod):
     _check(oracle_mod, recs, r, n=12)
 
 
+@pytest.mark.parametrize("seed", range(12456, 12466))
+def test_reference_integrity_batches(engine, oracle_mod, seed):
+    """AlgorithmCorrectnessTestProject/IntegrityTest.cs:62-87: 2^17 automata of
+    13 states from Problem.FillArrayOfProblems with seeds 12456..12465."""
+    from sbfs import dotnet_random as D
+    recs = D.fill_array_of_problems(1 << 17, 13, seed, lstride=13)
+    r = engine.solve(recs, n=13, lstride=13)
+    _check(oracle_mod, recs, r, n=13, lstride=13)
+
+
+def test_reference_benchmark_batch(engine, oracle_mod):
+    """The batch GPGPU/Program.cs:94 times for 2^20 automata at n = 12 (seed
+    1234567 + 2^20), in tight 24-byte records."""
+    from sbfs import dotnet_random as D
+    count = 1 << 20
+    recs = D.benchmark_batch(count, 12, lstride=12)
+    r = engine.solve(recs, n=12, lstride=12)
+    _check(oracle_mod, recs, r, n=12, lstride=12)
+    v = engine.verify(recs, n=12, lstride=12)
+    np.testing.assert_array_equal(v["len"], r["len"])
+    assert v["first_violation"] == -1
+
+
 def test_tight_records_same_as_64_byte_records(engine):
     recs = P.uniform_maps(50_000, 12, 42)
     a = engine.solve(recs, n=12, words=False)
