@@ -5,7 +5,10 @@
 
 Default workload (the benchmark's headline configuration): 1,000,000 uniform
 random binary automata with n = 12 states per GPU, tight 24-byte records,
-seeded synthetic inputs.  One step = one pass of the power-set BFS over the
+seeded synthetic inputs.  By default the n12 and n8 batches are the
+reference's own: Problem.FillArrayOfProblems with .NET System.Random and the
+benchmark's seed 1234567 + count (rank r > 0 adds 7919 * r); --inputs hash
+draws them from a counter hash instead.  One step = one pass of the power-set BFS over the
 whole batch, producing every shortest length (or the non-synchronizing flag)
 and one shortest word per automaton.
 
@@ -58,6 +61,8 @@ def parse_args():
     ap.add_argument("--rates", default="2000,8000,32000,128000,0",
                     help="serving: offered request rates per second (0 = submit all at once)")
     ap.add_argument("--count", type=int, default=0, help="automata per GPU (0 = the workload's size)")
+    ap.add_argument("--inputs", choices=["reference", "hash"], default="reference",
+                    help="n12/n8: the reference's System.Random batch or a counter-hash batch")
     ap.add_argument("--cpu-seconds", type=float, default=1.5, help="wall time of the CPU baseline sample")
     ap.add_argument("--plain-sample", type=int, default=2000)
     ap.add_argument("--no-e2e", action="store_true")
@@ -74,20 +79,30 @@ def parse_args():
 # workloads
 # ---------------------------------------------------------------------------
 
-def make_workload(name: str, count: int, rank: int, large_n=(24, 26, 28), kinds=("random", "cerny", "perm")):
+def _uniform_batch(count: int, n: int, rank: int, inputs: str, hash_seed: int):
+    from sbfs import dotnet_random as D
+    from sbfs import problem as P
+    if inputs == "reference":
+        seed = D.BENCHMARK_SEED + count + 7919 * rank
+        return D.fill_array_of_problems(count, n, seed, lstride=n), f"System.Random, seed {seed}"
+    return P.repack(P.uniform_maps(count, n, hash_seed + 1000 * rank), 32, n), f"counter hash 0x{hash_seed:X}"
+
+
+def make_workload(name: str, count: int, rank: int, large_n=(24, 26, 28), kinds=("random", "cerny", "perm"),
+                  inputs: str = "reference"):
     import numpy as np
     from sbfs import problem as P
 
     seed_base = 0x5EED
     if name == "n12":
         count = count or 1_000_000
-        recs = P.repack(P.uniform_maps(count, 12, seed_base + 1 + 1000 * rank), 32, 12)
-        return dict(recs=recs, ns=None, n=12, lstride=12, max_n=12, count=count,
+        recs, seed = _uniform_batch(count, 12, rank, inputs, seed_base + 1)
+        return dict(recs=recs, ns=None, n=12, lstride=12, max_n=12, count=count, seed=seed,
                     desc=f"batched uniform: {count:,} random binary automata, n=12, lengths + shortest words")
     if name == "n8":
         count = count or 10_000
-        recs = P.repack(P.uniform_maps(count, 8, seed_base + 0 + 1000 * rank), 32, 8)
-        return dict(recs=recs, ns=None, n=8, lstride=8, max_n=8, count=count,
+        recs, seed = _uniform_batch(count, 8, rank, inputs, seed_base + 0)
+        return dict(recs=recs, ns=None, n=8, lstride=8, max_n=8, count=count, seed=seed,
                     desc=f"plain config: {count:,} random binary automata, n=8")
     if name == "mixed":
         count = count or 200_000
@@ -95,7 +110,7 @@ def make_workload(name: str, count: int, rank: int, large_n=(24, 26, 28), kinds=
         recs = P.uniform_maps(count, ns, seed_base + 2 + 1000 * rank)
         for i in range(0, count, 100):   # 1% Cerny family
             recs[i] = P.cerny_record(int(ns[i]))
-        return dict(recs=recs, ns=ns, n=0, lstride=32, max_n=20, count=count,
+        return dict(recs=recs, ns=ns, n=0, lstride=32, max_n=20, count=count, seed="counter hash 0x5EED",
                     desc=f"batched mixed: {count:,} automata, n uniform in 6..20, 1% Cerny family")
     if name == "large":
         rows, ns = [], []
@@ -111,7 +126,7 @@ def make_workload(name: str, count: int, rank: int, large_n=(24, 26, 28), kinds=
         recs = np.stack(rows)
         ns = np.array(ns, dtype=np.uint8)
         return dict(recs=recs, ns=ns, n=0, lstride=32, max_n=max(large_n), count=len(ns),
-                    desc=f"large single instances: n={','.join(map(str, large_n))} x "
+                    seed="counter hash 0x5EED", desc=f"large single instances: n={','.join(map(str, large_n))} x "
                          f"({' + '.join(kinds)})")
     raise ValueError(name)
 
@@ -196,7 +211,7 @@ def run_reference(args):
     if rank != 0:
         return 0
     wl = make_workload(args.workload, args.count, 0, tuple(int(x) for x in args.large_n.split(",")),
-                       tuple(args.large_kinds.split(",")))
+                       tuple(args.large_kinds.split(",")), args.inputs)
     threads = os.cpu_count() or 1
     import oracle
 
@@ -213,7 +228,7 @@ def run_reference(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u16", "data": "synthetic", "impl": "reference",
-        "config": {"workload": wl["desc"], "automata": wl["count"], "n": wl["n"] or "6..28"},
+        "config": {"workload": wl["desc"], "automata": wl["count"], "n": wl["n"] or "6..28", "seed": wl["seed"]},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{args.steps} passes over the full {wl['count']:,}-automaton batch "
                                    f"({kind}, C restatement; the C# reference cannot run here)"},
@@ -261,7 +276,7 @@ def run_sbfs(args):
         torch.cuda.set_device(0)
     dev = torch.device("cuda", torch.cuda.current_device())
     wl = make_workload(args.workload, args.count, rank, tuple(int(x) for x in args.large_n.split(",")),
-                       tuple(args.large_kinds.split(",")))
+                       tuple(args.large_kinds.split(",")), args.inputs)
     count, lstride = wl["count"], wl["lstride"]
     ws = sbfs.word_stride_for(wl["max_n"])
     import tempfile
@@ -407,7 +422,7 @@ def run_sbfs(args):
                        "record_bytes": rec_bytes, "word_stride_u64": ws, "kernel": kernel,
                        "l2": "flushed by a 256 MiB write before every timed step",
                        "parallelism": f"{world} GPU(s), automata sharded by rank, no collective on the data path",
-                       "seed": "0x5EED-based counter hash"},
+                       "seed": wl["seed"]},
             "e2e": e2e,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "traffic": traffic,

@@ -41,6 +41,26 @@ struct Problem {
         return p;
     }
 
+    // Problem.FillArrayOfProblems (Problem.cs:32-39): `count` automata of n
+    // states from .NET System.Random(seed), bit for bit (sbfs_generate_reference_batch).
+    static std::vector<Problem> FillArrayOfProblems(int count, int n, int seed)
+    {
+        const int lstride = 32;
+        std::vector<uint8_t> recs((size_t)std::max(count, 0) * 2 * lstride);
+        const sbfs_status st = sbfs_generate_reference_batch(count, n, seed, recs.data(), lstride);
+        if (st != SBFS_OK) throw std::invalid_argument(sbfs_status_string(st));
+        std::vector<Problem> out((size_t)count);
+        for (int i = 0; i < count; ++i) {
+            Problem &p = out[(size_t)i];
+            p.size = n;
+            p.stateTransitioningMatrixA.assign(recs.begin() + (size_t)i * 2 * lstride,
+                                               recs.begin() + (size_t)i * 2 * lstride + n);
+            p.stateTransitioningMatrixB.assign(recs.begin() + (size_t)i * 2 * lstride + lstride,
+                                               recs.begin() + (size_t)i * 2 * lstride + lstride + n);
+        }
+        return out;
+    }
+
     // Problem.ToString (Problem.cs:60-79): "[[a0,a1,..],[b0,b1,..]]"
     std::string ToString() const
     {
