@@ -68,6 +68,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default kernel shapes")
     ap.add_argument("--no-graph", action="store_true", help="launch every step directly, no CUDA graphs")
+    ap.add_argument("--chunk", type=int, default=0, help="host path: automata per chunk (0 = library default)")
+    ap.add_argument("--streams", type=int, default=0, help="host path: chunks in flight (0 = library default)")
     ap.add_argument("--large-n", default="24,26,28", help="large workload: the state counts to include")
     ap.add_argument("--large-kinds", default="random,cerny,perm",
                     help="large workload: which families to include (random, cerny, perm)")
@@ -282,7 +284,8 @@ def run_sbfs(args):
     import tempfile
     tune_cache = os.path.join(tempfile.gettempdir(), "sbfs_tune_cache.txt")
     eng = sbfs.Engine(device=dev.index, autotune=not args.no_tune, tune_cache=tune_cache,
-                      use_graph=not args.no_graph, level_arena_bytes=args.level_arena_mb << 20)
+                      use_graph=not args.no_graph, level_arena_bytes=args.level_arena_mb << 20,
+                      chunk=args.chunk, streams=args.streams)
     plan = eng.plan()   # runs the autotuner (or reads its cache) before any timing
 
     def barrier():

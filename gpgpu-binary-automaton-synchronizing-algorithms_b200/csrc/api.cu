@@ -305,6 +305,10 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
            "launching escalation kernel");
         *launches += 1;
     }
+    if (!plain && j.len && j.count > 0) {
+        CK(launch_count_sync(j.len, j.count, &ctr->synchronizing, h->sm_count, st), "launching result count");
+        *launches += 1;
+    }
     return SBFS_OK;
 }
 
@@ -414,6 +418,7 @@ struct Totals {
     int64_t first_violation = -1;
     int64_t expanded = 0;
     int64_t escalated = 0;
+    int64_t synchronizing = 0;
     int error = 0;
     double kernel_ms = 0;
 };
@@ -427,6 +432,7 @@ sbfs_status finish_lane(sbfs_handle *h, Lane &L, Totals &t)
     t.error |= c->error;
     t.expanded += (int64_t)c->expanded;
     t.escalated += (int64_t)c->escal_range[1];
+    t.synchronizing += (int64_t)c->synchronizing;
     if (c->first_violation != ULLONG_MAX) {
         const int64_t g = L.begin + (int64_t)c->first_violation;
         if (t.first_violation < 0 || g < t.first_violation) t.first_violation = g;
@@ -580,13 +586,18 @@ sbfs_status solve_host(sbfs_handle *h, const uint8_t *maps, int32_t lstride, con
               word_stride};
         h2d += cnt * rec + (ns ? cnt : 0);
         d2h += (out_len ? cnt * (int64_t)sizeof(int32_t) : 0) + (int64_t)wb;
+        if (!plain) {
+            // records in on the shared copy stream (chunk order), then the lane waits for them
+            CK(cudaMemcpyAsync(L.maps.ptr, src_maps, cnt * rec, cudaMemcpyHostToDevice, h->copy_in),
+               "copying records");
+            if (ns) CK(cudaMemcpyAsync(L.ns.ptr, src_ns, cnt, cudaMemcpyHostToDevice, h->copy_in), "copying sizes");
+            CK(cudaEventRecord(L.ev_in, h->copy_in), "recording event");
+            CK(cudaStreamWaitEvent(L.stream, L.ev_in, 0), "ordering streams");
+        }
         CK(cudaEventRecord(L.ev_k0, L.stream), "recording event");
         if (!plain) {
-            // one chunk: copies in, counters, bucketing, class kernels, copies out
+            // one chunk: counters, bucketing, class kernels, copies out
             auto body = [&]() -> sbfs_status {
-                CK(cudaMemcpyAsync(L.maps.ptr, src_maps, cnt * rec, cudaMemcpyHostToDevice, L.stream),
-                   "copying records");
-                if (ns) CK(cudaMemcpyAsync(L.ns.ptr, src_ns, cnt, cudaMemcpyHostToDevice, L.stream), "copying sizes");
                 sbfs_status bs = reset_counters(h, L);
                 if (bs) return bs;
                 if ((bs = enqueue_kernels(h, L, j, &launches))) return bs;
@@ -658,9 +669,11 @@ sbfs_status solve_host(sbfs_handle *h, const uint8_t *maps, int32_t lstride, con
     if (stats) {
         stats->automata = count;
         stats->expanded = tot.expanded;
-        stats->synchronizing = 0;
-        if (out_len)
+        stats->synchronizing = tot.synchronizing;
+        if (plain && out_len) {
+            stats->synchronizing = 0;
             for (int64_t i = 0; i < count; ++i) stats->synchronizing += out_len[i] >= 0;
+        }
         stats->h2d_bytes = h2d;
         stats->d2h_bytes = d2h;
         stats->launches = launches;
@@ -751,14 +764,26 @@ sbfs_status sbfs_create(const sbfs_config *cfg, sbfs_handle **out)
     h->cfg = c;
     h->lanes.resize(c.streams > 0 ? std::min(c.streams, 16) : kDefaultLanes);
     if ((e = cudaEventCreateWithFlags(&h->ev_device, cudaEventDisableTiming)) != cudaSuccess ||
-        (e = cudaEventCreate(&h->ev_dk0)) != cudaSuccess || (e = cudaEventCreate(&h->ev_dk1)) != cudaSuccess) {
+        (e = cudaEventCreate(&h->ev_dk0)) != cudaSuccess || (e = cudaEventCreate(&h->ev_dk1)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&h->copy_in, cudaStreamNonBlocking)) != cudaSuccess) {
         sbfs_destroy(h);
         return cuda_fail(nullptr, e, "creating events");
     }
+    // lane i runs chunks i, i + lanes, ...: earlier lanes get higher stream
+    // priority, so an older chunk's pending CTAs (its escalation pass) are
+    // scheduled ahead of a younger chunk's and chunks complete in order
+    int prio_least = 0, prio_greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest) != cudaSuccess) {
+        cudaGetLastError();
+        prio_least = prio_greatest = 0;
+    }
+    int lane_index = 0;
     for (auto &L : h->lanes) {
-        if ((e = cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        const int prio = std::min(prio_least, prio_greatest + lane_index++);
+        if ((e = cudaStreamCreateWithPriority(&L.stream, cudaStreamNonBlocking, prio)) != cudaSuccess ||
             (e = cudaEventCreate(&L.ev_k0)) != cudaSuccess || (e = cudaEventCreate(&L.ev_k1)) != cudaSuccess ||
-            (e = cudaEventCreateWithFlags(&L.ev_done, cudaEventDisableTiming)) != cudaSuccess) {
+            (e = cudaEventCreateWithFlags(&L.ev_done, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&L.ev_in, cudaEventDisableTiming)) != cudaSuccess) {
             sbfs_destroy(h);
             return cuda_fail(nullptr, e, "creating streams");
         }
@@ -781,8 +806,13 @@ sbfs_status sbfs_destroy(sbfs_handle *h)
         if (L.ev_k0) cudaEventDestroy(L.ev_k0);
         if (L.ev_k1) cudaEventDestroy(L.ev_k1);
         if (L.ev_done) cudaEventDestroy(L.ev_done);
+        if (L.ev_in) cudaEventDestroy(L.ev_in);
         if (L.level_ready) L.level.destroy();
         if (L.stream) cudaStreamDestroy(L.stream);
+    }
+    if (h->copy_in) {
+        cudaStreamSynchronize(h->copy_in);
+        cudaStreamDestroy(h->copy_in);
     }
     if (h->ev_device) cudaEventDestroy(h->ev_device);
     if (h->ev_dk0) cudaEventDestroy(h->ev_dk0);
@@ -910,6 +940,7 @@ sbfs_status sbfs_device_wait(sbfs_handle *h, sbfs_stats *stats)
         stats->automata = h->device_count;
         stats->expanded = (int64_t)c->expanded;
         stats->escalated = (int64_t)c->escal_range[1];
+        stats->synchronizing = (int64_t)c->synchronizing;
         stats->launches = h->device_launches;
         float ms = 0;
         if (cudaEventElapsedTime(&ms, h->ev_dk0, h->ev_dk1) == cudaSuccess) stats->kernel_ms = ms;

@@ -29,6 +29,9 @@ struct ClassScratch {
     int32_t *order;               // count entries
 };
 
+// Adds the number of non-negative lengths in len[0..count) to *out.
+cudaError_t launch_count_sync(const int32_t *d_len, int64_t count, unsigned long long *out, int sm_count,
+                              cudaStream_t st);
 cudaError_t launch_classify(const uint8_t *d_ns, int64_t count, ClassScratch sc, int sm_count,
                             cudaStream_t st);
 

@@ -62,7 +62,35 @@ __global__ void k_scatter(const uint8_t *ns, int64_t count, unsigned long long *
     }
 }
 
+// out += number of lengths >= 0 (synchronizing automata); one atomic per block
+__global__ void k_count_sync(const int32_t *len, int64_t count, unsigned long long *out)
+{
+    __shared__ unsigned int part[32];
+    unsigned int c = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count;
+         i += (int64_t)gridDim.x * blockDim.x)
+        c += __ldcg(len + i) >= 0;
+    c = __reduce_add_sync(kFull, c);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        unsigned int v = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0u;
+        v = __reduce_add_sync(kFull, v);
+        if (threadIdx.x == 0 && v) atomicAdd(out, (unsigned long long)v);
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_count_sync(const int32_t *d_len, int64_t count, unsigned long long *out, int sm_count,
+                              cudaStream_t st)
+{
+    const int threads = 256;
+    const int64_t want = (count + threads - 1) / threads;
+    const int blocks = (int)(want < 1 ? 1 : (want > 2 * sm_count ? 2 * sm_count : want));
+    k_count_sync<<<blocks, threads, 0, st>>>(d_len, count, out);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_classify(const uint8_t *d_ns, int64_t count, ClassScratch sc, int sm_count,
                             cudaStream_t st)

@@ -15,11 +15,13 @@
 // entry carries the letters of the word that reaches it (bit NMAX + d =
 // letter d, 1 = b), so a word needs no parent pointers or retained history.
 //
-// Each iteration a lane takes up to two subsets of its current level.  Their
-// four images are tested in queue order (first subset's a, b, then the
-// second's), exactly as the sequential loop would; the four bitmap words are
-// loaded up front and a word touched twice is forwarded in registers, so the
-// test-and-sets do not wait on one another's shared-memory round trips.
+// Each iteration a lane takes up to two subsets of its current level and looks
+// up their four images.  A singleton among them ends the search (no singleton
+// is visited before the first one is generated, so it needs no bitmap test).
+// Otherwise the four images are test-and-set with shared-memory atomicOr, issued
+// back to back and kept in program order by the hardware for a repeated
+// address, and the fresh ones are appended in queue order (first subset's a, b,
+// then the second's), as the sequential loop would.
 //
 // Two rare cases leave this kernel: a frontier wider than R, and (with words)
 // a word longer than 32 - NMAX letters.  Such an automaton is abandoned and
@@ -197,56 +199,59 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
 
         // ---- up to two expansions per active lane ----------------------------
         if (state == kActive) {
+            // a lane with one subset left in the level expands it twice: the
+            // second copy's images are already visited by the time they are tested
             const bool two = head + 1u < lvl_end;
             const uint32_t e0 = rq[(head & rmask) * 32];
-            const uint32_t e1 = two ? rq[((head + 1u) & rmask) * 32] : 0u;
+            const uint32_t e1 = two ? rq[((head + 1u) & rmask) * 32] : e0;
             head += two ? 2u : 1u;
             expanded += two ? 2u : 1u;
             const uint32_t t0 = lane_image<NMAX>(tb, e0 & G::kMask);
             const uint32_t t1 = lane_image<NMAX>(tb, e1 & G::kMask);
             const uint32_t y[4] = {t0 >> 16, t0 & 0xFFFFu, t1 >> 16, t1 & 0xFFFFu};
-            uint32_t wd[4], mk[4], wv[4];
+            // entries carry the word that reaches them: the parent's letters,
+            // plus letter `level` = b for the b-images (an entry holds 32 - NMAX
+            // letters; at level >= 32 - NMAX a fresh image escalates instead)
+            const uint32_t lb = (WORDS && level < (uint32_t)G::kWordMax) ? 1u << (level + NMAX) : 0u;
+            const uint32_t hi[4] = {WORDS ? (e0 & ~G::kMask) : 0u, WORDS ? ((e0 & ~G::kMask) | lb) : 0u,
+                                    WORDS ? (e1 & ~G::kMask) : 0u, WORDS ? ((e1 & ~G::kMask) | lb) : 0u};
+            // no singleton is ever visited (the search stops at the first one), so
+            // a singleton image ends the search without a bitmap test
+            int sc = -1;
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                wd[c] = y[c] >> 5;
-                mk[c] = 1u << (y[c] & 31u);
-                wv[c] = (c < 2 || two) ? bm[wd[c] * 32] : kFull;
-            }
-            bool stop = false;
-            bool pushed[4] = {false, false, false, false};
+            for (int c = 3; c >= 0; --c)
+                if (is_singleton(y[c])) sc = c;
+            if (sc >= 0) {
+                state = kDone;
+                res_len = (int32_t)level + 1;
+                res_word = WORDS ? (((sc < 2 ? e0 : e1) >> NMAX) | ((uint32_t)(sc & 1) << level)) : 0u;
+            } else {
+                // test-and-set in queue order: a subset met twice in this step is
+                // fresh only the first time (same-address atomics keep program order)
+                uint32_t old[4];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                // bits set earlier in this iteration in the same bitmap word
+                for (int c = 0; c < 4; ++c) old[c] = atomicOr(&bm[(y[c] >> 5) * 32], 1u << (y[c] & 31u));
+                bool any = false;
 #pragma unroll
-                for (int p = 0; p < c; ++p)
-                    if (pushed[p] && wd[p] == wd[c]) wv[c] |= mk[p];
-                const bool fresh = !stop && !(wv[c] & mk[c]);
-                const uint32_t wbits = WORDS ? ((c < 2 ? e0 : e1) >> NMAX) : 0u;
-                const uint32_t letter = (uint32_t)(c & 1);
-                if (fresh && is_singleton(y[c])) {
-                    stop = true;
-                    state = kDone;
-                    res_len = (int32_t)level + 1;
-                    res_word = WORDS ? (wbits | (letter << level)) : 0u;
-                } else if (fresh) {
-                    if (tail - head >= (uint32_t)ring || (WORDS && level >= (uint32_t)G::kWordMax)) {
-                        stop = true;
-                        state = kEscalate;
-                    } else {
-                        pushed[c] = true;
-                        bm[wd[c] * 32] = wv[c] | mk[c];
-                        rq[(tail & rmask) * 32] = WORDS ? (y[c] | ((wbits | (letter << level)) << NMAX)) : y[c];
+                for (int c = 0; c < 4; ++c) {
+                    if (!(old[c] & (1u << (y[c] & 31u)))) {
+                        rq[(tail & rmask) * 32] = y[c] | hi[c];
                         ++tail;
+                        any = true;
                     }
                 }
-            }
-            if (!stop && head == lvl_end) {
-                if (tail == lvl_end) {
-                    state = kDone;
-                    res_len = kLenNonSync;
-                } else {
-                    lvl_end = tail;
-                    ++level;
+                // more live entries than ring slots (the oldest were overwritten), or
+                // a word longer than an entry carries: the pooled kernel takes over
+                if (tail - head > (uint32_t)ring || (WORDS && any && level >= (uint32_t)G::kWordMax)) {
+                    state = kEscalate;
+                } else if (head == lvl_end) {
+                    if (tail == lvl_end) {
+                        state = kDone;
+                        res_len = kLenNonSync;
+                    } else {
+                        lvl_end = tail;
+                        ++level;
+                    }
                 }
             }
         }

@@ -26,6 +26,7 @@ struct DevCounters {
     unsigned long long escal_range[2];            // {0, automata appended to the escalation list}
     int error;
     int pad;
+    unsigned long long synchronizing;             // lengths >= 0 written by this job
 };
 
 // Grow-only device allocation.
@@ -65,6 +66,7 @@ struct CtaShape {
 struct Lane {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr, ev_done = nullptr;
+    cudaEvent_t ev_in = nullptr;               // this lane's records have arrived (host path)
     DevBuf maps, ns, len, words, spill, order, counters, ranges, cta_queue, hbm_bitmap, hbm_queue,
         escal, tickets;
     LevelEngine level;                         // device-resident slots for n > 20
@@ -134,6 +136,10 @@ struct sbfs_handle {
     std::string last_error;
     std::mutex mu;
     std::vector<sbfs::Lane> lanes;
+    // host path: every chunk's records go host->device on this one stream, in
+    // chunk order, so the first chunk's kernels start after one chunk's copy
+    // rather than after all lanes' copies have shared the link
+    cudaStream_t copy_in = nullptr;
     sbfs::Plan plan{};
     bool plan_ready = false;
     // last sbfs_solve_batch_device call: lane 0's buffers are in use until ev_device

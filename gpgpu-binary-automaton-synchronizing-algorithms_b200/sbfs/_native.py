@@ -1,8 +1,9 @@
 """ctypes binding of libsbfs.so (include/sbfs.h).
 
-The library is loaded from ``sbfs/_lib/libsbfs.so`` inside this package; there
-is no fallback: if the library is missing or cannot be loaded, every call
-raises ``NativeUnavailable``.
+The library is loaded from ``sbfs/_lib/libsbfs.so`` inside this package (or
+from the path in the ``SBFS_LIB`` environment variable); there is no
+fallback: if the library is missing or cannot be loaded, every call raises
+``NativeUnavailable``.
 """
 from __future__ import annotations
 
@@ -11,7 +12,8 @@ import os
 from typing import Optional
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_lib", "libsbfs.so")
+# SBFS_LIB may name another build of the same library (e.g. an installed copy)
+LIB_PATH = os.environ.get("SBFS_LIB") or os.path.join(HERE, "_lib", "libsbfs.so")
 
 # every symbol include/sbfs.h declares (checked by the CPU test suite)
 EXPORTS = [

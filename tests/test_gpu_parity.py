@@ -18,6 +18,8 @@ def _check(oracle_mod, recs, r, ns=None, n=0, lstride=32, ref=None):
     if ref is None:
         ref = oracle_mod.solve(recs, ns=ns, n=n, lstride=lstride, words=False, threads=8)
     np.testing.assert_array_equal(r["len"], ref["len"])
+    if "stats" in r:
+        assert r["stats"]["synchronizing"] == int((ref["len"] >= 0).sum())
     if r.get("words") is not None:
         bad, ok = oracle_mod.replay(recs, r["len"], r["words"], ns=ns, n=n, lstride=lstride)
         assert bad == 0, np.nonzero(ok != 3)[0][:10]
@@ -202,6 +204,7 @@ def test_device_buffer_path(engine, oracle_mod):
     st = engine.wait_device()
     assert st["automata"] == len(ns) and st["launches"] >= 3
     lens = d_len.cpu().numpy()
+    assert st["synchronizing"] == int((lens >= 0).sum())
     ref = oracle_mod.solve(recs, ns=ns, words=False, threads=8)
     np.testing.assert_array_equal(lens, ref["len"])
     assert int(d_fv.item()) == -1
@@ -228,6 +231,8 @@ def test_cuda_graph_replay_matches(oracle_mod):
             assert oracle_mod.replay(recs, r["len"], r["words"], n=12)[0] == 0
             m = eng.solve(mixed, ns=ns)
             np.testing.assert_array_equal(m["len"], ref_mixed)
+            assert r["stats"]["synchronizing"] == int((ref >= 0).sum())
+            assert m["stats"]["synchronizing"] == int((ref_mixed >= 0).sum())
         big = P.uniform_maps(300_000, 12, 904)   # larger chunks: buffers move, graphs rebuild
         with sbfs.Engine(device=0, use_graph=True, chunk=1 << 18) as eng2:
             for rep in range(3):
