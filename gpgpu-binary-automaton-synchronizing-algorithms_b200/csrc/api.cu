@@ -246,6 +246,7 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
     b.error = &ctr->error;
 
     const int present = class_present_mask(j);
+    const size_t escal_entries = (size_t)std::max<int64_t>(j.count, 1);
     if (j.ns) {
         CK(L.order.reserve((size_t)j.count * sizeof(int32_t)), "allocating order array");
         // hist[K] | ranges[2K] | cursor[K]
@@ -263,9 +264,12 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
         unsigned long long *ticket = ticket_override ? ticket_override : &ctr->ticket[c];
         if (c < 2 && !plain && !P.use_pool[c]) {
             const LaneShape &ls = P.lane[c];
-            CK(L.escal.reserve((size_t)std::max<int64_t>(j.count, 1) * sizeof(int32_t)), "allocating escalation list");
-            CK(launch_lane(ls.nmax, ls.warps, ls.ring, ls.refill_k, ls.ctas, bc, L.escal.as<int32_t>(),
-                           &ctr->escal_range[1], ticket, st),
+            // one escalation list per lane class; entries read as -1 until stored
+            CK(L.escal.reserve(2 * escal_entries * sizeof(int32_t)), "allocating escalation list");
+            int32_t *list = L.escal.as<int32_t>() + (size_t)c * escal_entries;
+            CK(cudaMemsetAsync(list, 0xFF, escal_entries * sizeof(int32_t), st), "resetting escalation list");
+            CK(launch_lane(ls.nmax, ls.warps, ls.ring, ls.refill_k, ls.ctas, bc, list, &ctr->escal_count[c],
+                           &ctr->escal_claim[c], &ctr->lane_drained[c], ticket, st),
                "launching per-lane kernel");
         } else if (c < 3) {
             const PoolShape &s = P.pool[c];
@@ -288,21 +292,6 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
             if (ls) return ls;
             continue;
         }
-        *launches += 1;
-    }
-    const bool lane_used = ((present & 1) && !P.use_pool[0]) || ((present & 2) && !P.use_pool[1]);
-    if (!plain && lane_used) {
-        // automata the per-lane kernel handed back (frontier wider than its ring,
-        // or a word longer than an entry carries) are the heavy tail: the pooled
-        // kernel with a deep on-chip queue and small work grabs spreads them out
-        Batch be = b;
-        be.ns = j.ns;
-        be.order = L.escal.as<int32_t>();
-        be.range_dev = ctr->escal_range;
-        const PoolShape &s = P.escal;
-        CK(L.spill.reserve(pool_spill_words(s) * sizeof(uint32_t)), "allocating queue spill");
-        CK(launch_pool(s, be, L.spill.as<uint32_t>(), &ctr->ticket[kNumClasses], st),
-           "launching escalation kernel");
         *launches += 1;
     }
     if (!plain && j.len && j.count > 0) {
@@ -342,9 +331,9 @@ sbfs_status ensure_plan(sbfs_handle *h)
         s.ctas = per_sm * sms;
     }
     const int lane_defaults[2][4] = {
-        // warps, ring, refill_k
+        // warps, ring, refill_k (the autotuner's picks on B200 for uniform n = 8 and n = 12)
         {8, 16, 16, 0},
-        {2, 32, 16, 0},
+        {1, 64, 16, 0},
     };
     for (int c = 0; c < 2; ++c) {
         LaneShape &ls = P.lane[c];
@@ -359,14 +348,6 @@ sbfs_status ensure_plan(sbfs_handle *h)
         const int per_sm = lane_max_ctas_per_sm(ls.nmax, ls.warps, ls.ring);
         if (per_sm < 1) return fail(h, SBFS_EINVAL, "per-lane kernel shape does not fit in shared memory");
         ls.ctas = per_sm * sms;
-    }
-    P.escal = PoolShape{12, h->cfg.escal_slots > 0 ? h->cfg.escal_slots : 4, 2,
-                        h->cfg.escal_queue > 0 ? h->cfg.escal_queue : 256, 1,
-                        h->cfg.escal_grab > 0 ? h->cfg.escal_grab : 4};
-    {
-        const int per_sm = pool_max_ctas_per_sm(P.escal);
-        if (per_sm < 1) return fail(h, SBFS_EINVAL, "escalation kernel shape does not fit in shared memory");
-        P.escal.ctas = per_sm * sms;
     }
     P.cta.threads = 512;
     P.cta.ctas = sms * 4;
@@ -431,7 +412,7 @@ sbfs_status finish_lane(sbfs_handle *h, Lane &L, Totals &t)
     const DevCounters *c = L.h_counters.as<DevCounters>();
     t.error |= c->error;
     t.expanded += (int64_t)c->expanded;
-    t.escalated += (int64_t)c->escal_range[1];
+    t.escalated += (int64_t)(c->escal_count[0] + c->escal_count[1]);
     t.synchronizing += (int64_t)c->synchronizing;
     if (c->first_violation != ULLONG_MAX) {
         const int64_t g = L.begin + (int64_t)c->first_violation;
@@ -939,7 +920,7 @@ sbfs_status sbfs_device_wait(sbfs_handle *h, sbfs_stats *stats)
         std::memset(stats, 0, sizeof(*stats));
         stats->automata = h->device_count;
         stats->expanded = (int64_t)c->expanded;
-        stats->escalated = (int64_t)c->escal_range[1];
+        stats->escalated = (int64_t)(c->escal_count[0] + c->escal_count[1]);
         stats->synchronizing = (int64_t)c->synchronizing;
         stats->launches = h->device_launches;
         float ms = 0;

@@ -17,6 +17,7 @@ constexpr int32_t kLenInvalid = -2;   // malformed record (state >= n); host tur
 // Device error bits (one int per launch set, read back by the host).
 constexpr int kErrInvalid = 1;        // malformed automaton seen
 constexpr int kErrCapacity = 2;       // a queue or frontier exceeded its reserved space
+constexpr int kErrWait = 4;           // a bounded wait for another warp's store ran out
 
 // Everything a BFS kernel needs to know about the batch.
 struct Batch {
@@ -95,8 +96,10 @@ int pool_max_ctas_per_sm(const PoolShape &s);
 
 size_t lane_smem_bytes(int nmax, int warps, int ring);
 int lane_max_ctas_per_sm(int nmax, int warps, int ring);
+// escal_list must hold -1 in every entry the launch may append (count
+// entries); escal_count, escal_claim and drained start at 0.
 cudaError_t launch_lane(int nmax, int warps, int ring, int refill_k, int ctas, const Batch &b,
-                        int32_t *escal_list, unsigned long long *escal_count, unsigned long long *ticket,
-                        cudaStream_t st);
+                        int32_t *escal_list, unsigned long long *escal_count, unsigned long long *escal_claim,
+                        unsigned int *drained, unsigned long long *ticket, cudaStream_t st);
 
 }  // namespace sbfs

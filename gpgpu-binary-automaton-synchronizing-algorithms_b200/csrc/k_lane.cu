@@ -23,10 +23,17 @@
 // address, and the fresh ones are appended in queue order (first subset's a, b,
 // then the second's), as the sequential loop would.
 //
-// Two rare cases leave this kernel: a frontier wider than R, and (with words)
-// a word longer than 32 - NMAX letters.  Such an automaton is abandoned and
-// appended to an escalation list that the warp-pooled kernel (k_pool.cu)
-// solves afterwards.
+// Two rare cases leave the per-lane search: a frontier wider than R, and (with
+// words) a word longer than 32 - NMAX letters.  Such an automaton is abandoned
+// and appended to the launch's escalation list.  A warp that has no lane work
+// left (no new automata, every lane idle) owns its whole shared-memory region
+// again and takes escalated automata from that list one at a time, solving
+// each with all 32 lanes: a level-synchronous search over a linear queue that
+// holds every subset at most once (2^n entries, so it cannot overflow), with
+// parent pointers for the word, the nibble table in registers read by warp
+// shuffles, and a linear bitmap updated with shared-memory atomics.  The last
+// warp to run out of lane work empties the list, so no escalated automaton is
+// left for another launch.
 //
 // Lanes that finish wait until `refill_k` lanes of the warp are idle; then the
 // warp writes their results and loads new automata for all of them in one
@@ -62,9 +69,143 @@ __device__ __forceinline__ uint32_t lane_image(const uint32_t *tb, uint32_t x)
     return t;
 }
 
+// Nibble-table entry v of chunk c (a-image << 16 | b-image of the states
+// 4c + i for the set bits i of v), read from the record.
+template <int NMAX>
+__device__ __forceinline__ uint32_t table_entry(const uint8_t *rec, int lstride, int n, int c, int v)
+{
+    uint32_t t = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int st = 4 * c + i;
+        if (((v >> i) & 1) && st < n)
+            t |= (1u << (__ldg(rec + st) + 16)) | (1u << __ldg(rec + lstride + st));
+    }
+    return t;
+}
+
+// Claims the next escalated automaton of the launch for a warp with no lane
+// work left, or returns -1 once there is none and none can come.  A claim is
+// one atomicAdd (never retried).  Its entry may not exist yet: it is appended
+// later by a warp still running lane work, or never, when every warp of the
+// launch has finished its lane work (each one fences its last append before it
+// counts itself in `drained`).  The writer bumps the count before it stores
+// the entry, so an entry is read until it is no longer -1.  All waits are
+// bounded (kErrWait on time-out).
+__device__ int64_t claim_escalated(const int32_t *list, const unsigned long long *count, unsigned long long *claim,
+                                   const unsigned int *drained, unsigned int warps, int *error)
+{
+    const unsigned long long pos = atomicAdd(claim, 1ull);
+    for (int it = 0; it < (1 << 22); ++it) {
+        if (pos < *(volatile const unsigned long long *)count) {
+            const int32_t v = *(volatile const int32_t *)(list + pos);
+            if (v >= 0) return v;
+        } else if (*(volatile const unsigned int *)drained >= warps) {
+            __threadfence();
+            if (pos >= *(volatile const unsigned long long *)count) return -1;
+            continue;
+        }
+        __nanosleep(100);
+    }
+    atomicOr(error, kErrWait);
+    return -1;
+}
+
+// One automaton (n <= NMAX) solved by the whole warp inside its region of
+// `region_words` shared words (>= 2^NMAX / 32 + 2^NMAX).  Queue entry:
+// subset | parent index << NMAX | letter << 2*NMAX (letter 1 = b).
+template <int NMAX, bool WORDS>
+__device__ void warp_solve(const Batch &b, int64_t k, uint32_t *region, int lane, unsigned long long &expanded)
+{
+    using G = LaneGeom<NMAX>;
+    constexpr int BW = G::kBitmapWords;
+    uint32_t *bm = region;        // linear bitmap
+    uint32_t *q = region + BW;    // linear queue, 2^NMAX entries
+    const int n = automaton_n(b, k);
+    const uint8_t *rec = b.maps + (size_t)k * 2u * (size_t)b.lstride;
+    // chunks 0 and 1 in lanes 0-15 / 16-31 of t01, chunk 2 in lanes 0-15 of t2
+    const uint32_t t01 = table_entry<NMAX>(rec, b.lstride, n, lane >> 4, lane & 15);
+    const uint32_t t2 = G::kChunks > 2 ? table_entry<NMAX>(rec, b.lstride, n, 2, lane & 15) : 0u;
+    for (int w = lane; w < BW; w += 32) bm[w] = 0u;
+    __syncwarp();
+    const uint32_t full = (1u << n) - 1u;
+    if (lane == 0) {
+        bm[full >> 5] = 1u << (full & 31u);
+        q[0] = full;
+    }
+    __syncwarp();
+    uint32_t head = 0, lvl_end = 1, tail = 1, level = 0;
+    int32_t len = kLenNonSync;
+    uint32_t found = 0, found_letter = 0;
+    while (true) {
+        const uint32_t idx = head + (uint32_t)lane;
+        const bool has = idx < lvl_end;
+        const uint32_t x = has ? (q[idx] & G::kMask) : 0u;
+        uint32_t t = __shfl_sync(kFull, t01, (int)(x & 15u)) | __shfl_sync(kFull, t01, 16 + (int)((x >> 4) & 15u));
+        if (G::kChunks > 2) t |= __shfl_sync(kFull, t2, (int)((x >> 8) & 15u));
+        const uint32_t ya = t >> 16, yb = t & 0xFFFFu;
+        expanded += has ? 1u : 0u;
+        const bool sa = has && is_singleton(ya), sb = has && is_singleton(yb);
+        const unsigned smask = __ballot_sync(kFull, sa || sb);
+        if (smask) {
+            // the first singleton in queue order (lowest lane, a before b)
+            const int fl = __ffs(smask) - 1;
+            found = head + (uint32_t)fl;
+            found_letter = (uint32_t)__shfl_sync(kFull, sa ? 0 : 1, fl);
+            len = (int32_t)level + 1;
+            break;
+        }
+        bool fa = false, fb = false;
+        if (has) {
+            fa = !(atomicOr(&bm[ya >> 5], 1u << (ya & 31u)) & (1u << (ya & 31u)));
+            fb = !(atomicOr(&bm[yb >> 5], 1u << (yb & 31u)) & (1u << (yb & 31u)));
+        }
+        const unsigned ma = __ballot_sync(kFull, fa), mb = __ballot_sync(kFull, fb);
+        const unsigned lt = (1u << lane) - 1u;
+        uint32_t pos = tail + (uint32_t)(__popc(ma & lt) + __popc(mb & lt));
+        const uint32_t par = idx << NMAX;
+        if (fa) q[pos++] = ya | par;
+        if (fb) q[pos] = yb | par | (1u << (2 * NMAX));
+        tail += (uint32_t)(__popc(ma) + __popc(mb));
+        head = min(head + 32u, lvl_end);
+        __syncwarp();
+        if (head == lvl_end) {
+            if (tail == lvl_end) break;   // no new subset: not synchronizing
+            lvl_end = tail;
+            ++level;
+        }
+    }
+    if (lane == 0) {
+        record_result(b, k, n, len);
+        if (WORDS) {
+            // letters from the root: entry at depth d + 1 holds letter d
+            uint64_t w0 = 0, w1 = 0;
+            if (len > 0) {
+                auto set = [&](uint32_t d) {
+                    if (d < 64) w0 |= 1ull << d;
+                    else if (d < 128) w1 |= 1ull << (d - 64);
+                };
+                if (found_letter) set(level);
+                uint32_t i = found;
+                for (int d = (int)level - 1; d >= 0; --d) {
+                    const uint32_t e = q[i];
+                    if ((e >> (2 * NMAX)) & 1u) set((uint32_t)d);
+                    i = (e >> NMAX) & G::kMask;
+                }
+            }
+            uint64_t *w = b.out_words + (size_t)k * (size_t)b.word_stride;
+            w[0] = w0;
+            if (b.word_stride > 1) w[1] = w1;
+            for (int c = 2; c < b.word_stride; ++c) w[c] = 0ull;
+        }
+    }
+    __syncwarp();
+}
+
 template <int NMAX, bool WORDS>
 __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, int32_t *escal_list,
-                                              unsigned long long *escal_count, unsigned long long *ticket)
+                                              unsigned long long *escal_count, unsigned long long *escal_claim,
+                                              unsigned int *drained, unsigned long long *ticket)
 {
     using G = LaneGeom<NMAX>;
     constexpr int BW = G::kBitmapWords;
@@ -192,7 +333,22 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
                 }
             }
             if (__ballot_sync(kFull, state == kActive) == 0u) {
-                if (!more) break;
+                if (!more) {
+                    // no lane work left: the region is free for escalated automata
+                    if (lane == 0) {
+                        __threadfence();   // this warp's appends before its count
+                        atomicAdd(drained, 1u);
+                    }
+                    const unsigned int warps = gridDim.x * (blockDim.x >> 5);
+                    while (true) {
+                        int64_t e = -1;
+                        if (lane == 0) e = claim_escalated(escal_list, escal_count, escal_claim, drained, warps, b.error);
+                        e = __shfl_sync(kFull, e, 0);
+                        if (e < 0) break;
+                        warp_solve<NMAX, WORDS>(b, e, base, lane, expanded);
+                    }
+                    break;
+                }
                 continue;
             }
         }
@@ -269,12 +425,17 @@ size_t smem_for(int warps, int ring)
 
 template <int NMAX, bool WORDS>
 cudaError_t launch_t(int warps, int ring, int refill_k, int ctas, const Batch &b, int32_t *escal_list,
-                     unsigned long long *escal_count, unsigned long long *ticket, cudaStream_t st)
+                     unsigned long long *escal_count, unsigned long long *escal_claim, unsigned int *drained,
+                     unsigned long long *ticket, cudaStream_t st)
 {
+    using G = LaneGeom<NMAX>;
+    // the warp-cooperative search needs the bitmap and 2^NMAX queue entries in one region
+    static_assert(G::kTable * 32 >= G::kBitmapWords, "region too small for the warp search");
     const size_t smem = smem_for<NMAX>(warps, ring);
     cudaError_t e = cudaFuncSetAttribute(k_lane<NMAX, WORDS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_lane<NMAX, WORDS><<<ctas, warps * 32, smem, st>>>(b, ring, refill_k, escal_list, escal_count, ticket);
+    k_lane<NMAX, WORDS><<<ctas, warps * 32, smem, st>>>(b, ring, refill_k, escal_list, escal_count, escal_claim,
+                                                       drained, ticket);
     return cudaGetLastError();
 }
 
@@ -302,18 +463,22 @@ int lane_max_ctas_per_sm(int nmax, int warps, int ring)
 }
 
 cudaError_t launch_lane(int nmax, int warps, int ring, int refill_k, int ctas, const Batch &b,
-                        int32_t *escal_list, unsigned long long *escal_count, unsigned long long *ticket,
-                        cudaStream_t st)
+                        int32_t *escal_list, unsigned long long *escal_count, unsigned long long *escal_claim,
+                        unsigned int *drained, unsigned long long *ticket, cudaStream_t st)
 {
     if ((ring & (ring - 1)) || ring < 8 || warps < 1 || warps > 8 || ctas < 1 || refill_k < 1 || refill_k > 32)
         return cudaErrorInvalidValue;
     const bool words = b.out_words != nullptr;
     if (nmax <= 8)
-        return words ? launch_t<8, true>(warps, ring, refill_k, ctas, b, escal_list, escal_count, ticket, st)
-                     : launch_t<8, false>(warps, ring, refill_k, ctas, b, escal_list, escal_count, ticket, st);
+        return words ? launch_t<8, true>(warps, ring, refill_k, ctas, b, escal_list, escal_count, escal_claim,
+                                         drained, ticket, st)
+                     : launch_t<8, false>(warps, ring, refill_k, ctas, b, escal_list, escal_count, escal_claim,
+                                          drained, ticket, st);
     if (nmax <= 12)
-        return words ? launch_t<12, true>(warps, ring, refill_k, ctas, b, escal_list, escal_count, ticket, st)
-                     : launch_t<12, false>(warps, ring, refill_k, ctas, b, escal_list, escal_count, ticket, st);
+        return words ? launch_t<12, true>(warps, ring, refill_k, ctas, b, escal_list, escal_count, escal_claim,
+                                          drained, ticket, st)
+                     : launch_t<12, false>(warps, ring, refill_k, ctas, b, escal_list, escal_count, escal_claim,
+                                           drained, ticket, st);
     return cudaErrorInvalidValue;
 }
 

@@ -20,10 +20,14 @@ namespace sbfs {
 
 // Counters one launch sequence reads and writes on the device.
 struct DevCounters {
-    unsigned long long ticket[kNumClasses + 1];   // per-class work tickets (+ escalation list)
+    unsigned long long ticket[kNumClasses + 1];   // per-class work tickets (last one spare)
     unsigned long long first_violation;
     unsigned long long expanded;
-    unsigned long long escal_range[2];            // {0, automata appended to the escalation list}
+    // per-lane kernels of classes 0 and 1: automata appended to the class's
+    // escalation list, claims on it, warps done with their lane work
+    unsigned long long escal_count[2];
+    unsigned long long escal_claim[2];
+    unsigned int lane_drained[2];
     int error;
     int pad;
     unsigned long long synchronizing;             // lengths >= 0 written by this job
@@ -113,7 +117,6 @@ struct Plan {
     CtaShape cta;
     CtaShape hbm;
     int use_pool[2];     // classes 0, 1: 1 = warp-pooled kernel instead of one automaton per lane
-    PoolShape escal;     // pooled kernel shape for automata the per-lane kernel handed back
     int class3_level;    // class 3: 1 = bitmaps in HBM (level slots) instead of shared memory (k_cta)
     int tuned;           // 1 when the autotuner (or its cache) chose the shapes
 };

@@ -79,8 +79,8 @@ std::string device_key(sbfs_handle *h)
 {
     cudaDeviceProp p;
     cudaGetDeviceProperties(&p, h->device);
-    char buf[256];
-    std::snprintf(buf, sizeof buf, "%s|sm%d|abi%d|v4", p.name, h->sm_count, SBFS_ABI_VERSION);
+    char buf[320];
+    std::snprintf(buf, sizeof buf, "%s|sm%d|abi%d|v5", p.name, h->sm_count, SBFS_ABI_VERSION);
     for (char *c = buf; *c; ++c)
         if (*c == ' ') *c = '_';
     return buf;
@@ -119,13 +119,6 @@ bool finish_shapes(sbfs_handle *h, Plan &P)
         const int per = lane_max_ctas_per_sm(P.lane[c].nmax, P.lane[c].warps, P.lane[c].ring);
         if (per < 1) return false;
         P.lane[c].ctas = per * h->sm_count;
-    }
-    {
-        PoolShape s = P.escal;
-        s.ctas = 1;
-        const int per = pool_max_ctas_per_sm(s);
-        if (per < 1) return false;
-        P.escal.ctas = per * h->sm_count;
     }
     for (int c = 0; c < 3; ++c) {
         PoolShape s = P.pool[c];

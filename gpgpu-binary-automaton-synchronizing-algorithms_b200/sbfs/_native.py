@@ -56,9 +56,6 @@ class Config(ctypes.Structure):
         ("lane_refill", ctypes.c_int32),
         ("lane_warps", ctypes.c_int32),
         ("streams", ctypes.c_int32),
-        ("escal_slots", ctypes.c_int32),
-        ("escal_queue", ctypes.c_int32),
-        ("escal_grab", ctypes.c_int32),
         ("level_arena_bytes", ctypes.c_int64),
         ("tune_cache", ctypes.c_char_p),
     ]

@@ -39,7 +39,7 @@ class Engine:
     def __init__(self, device: int = -1, slack: int = 0, autotune: bool = False, use_graph: bool = False,
                  slots_per_warp: int = 0, warps_per_cta: int = 0, queue_smem: int = 0, chunk: int = 0,
                  small_kernel: int = 0, lane_ring: int = 0, lane_refill: int = 0, lane_warps: int = 0,
-                 streams: int = 0, escal_slots: int = 0, escal_queue: int = 0, escal_grab: int = 0,
+                 streams: int = 0,
                  level_arena_bytes: int = 0, tune_cache: Optional[str] = None):
         self.lib = _native.load()
         cfg = _native.Config()
@@ -57,9 +57,6 @@ class Engine:
         cfg.lane_refill = lane_refill
         cfg.lane_warps = lane_warps
         cfg.streams = streams
-        cfg.escal_slots = escal_slots
-        cfg.escal_queue = escal_queue
-        cfg.escal_grab = escal_grab
         cfg.level_arena_bytes = level_arena_bytes
         self._tune_cache = tune_cache.encode() if tune_cache else None
         cfg.tune_cache = self._tune_cache

@@ -87,9 +87,6 @@ typedef struct sbfs_config {
     int32_t lane_refill;       /* per-lane kernel: idle lanes that trigger a refill; 0 = auto */
     int32_t lane_warps;        /* per-lane kernel: warps per CTA; 0 = auto              */
     int32_t streams;           /* streams the host path rotates chunks over; 0 = 4      */
-    int32_t escal_slots;       /* heavy-tail pass: automata per warp; 0 = auto          */
-    int32_t escal_queue;       /* heavy-tail pass: on-chip queue entries; 0 = auto      */
-    int32_t escal_grab;        /* heavy-tail pass: automata per work ticket; 0 = auto   */
     int64_t level_arena_bytes; /* HBM budget of the n > 20 level slots; 0 = half of free memory, <= 64 GiB */
     const char *tune_cache;    /* autotuner cache file, or NULL for in-memory only      */
 } sbfs_config;
@@ -104,7 +101,7 @@ typedef struct sbfs_stats {
     int32_t classes;           /* size classes used (small / cta / hbm)                 */
     double kernel_ms;          /* device time of the BFS kernels (CUDA events)          */
     double total_ms;           /* wall time of the call                                 */
-    int64_t escalated;         /* automata the per-lane kernel handed to the pooled one */
+    int64_t escalated;         /* automata the per-lane search handed to a whole warp   */
 } sbfs_stats;
 
 SBFS_API int32_t sbfs_abi_version(void);

@@ -32,9 +32,12 @@ def test_config1_plain_n8(engine, oracle_mod):
     r = engine.solve(recs, n=8)
     ref = _check(oracle_mod, recs, r, n=8)
     assert (r["len"] > 49).sum() == 0
-    # the GPU finishes the step in which the first singleton appears, the
-    # sequential oracle stops at that singleton: never fewer expansions
-    assert r["stats"]["expanded"] >= ref["expanded"]
+    # the GPU finishes the step in which the first singleton appears while the
+    # sequential oracle stops at that singleton (more expansions), but a warp
+    # sharing one heavy automaton may meet a singleton earlier within the last
+    # level than the sequential order does (fewer): the totals stay close
+    ratio = r["stats"]["expanded"] / ref["expanded"]
+    assert 0.95 <= ratio <= 1.5, ratio
 
 
 def test_config2_n12_full_batch_and_sample(engine, oracle_mod):
