@@ -268,8 +268,8 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
             CK(L.escal.reserve(2 * escal_entries * sizeof(int32_t)), "allocating escalation list");
             int32_t *list = L.escal.as<int32_t>() + (size_t)c * escal_entries;
             CK(cudaMemsetAsync(list, 0xFF, escal_entries * sizeof(int32_t), st), "resetting escalation list");
-            CK(launch_lane(ls.nmax, ls.warps, ls.ring, ls.refill_k, ls.ctas, bc, list, &ctr->escal_count[c],
-                           &ctr->escal_claim[c], &ctr->lane_drained[c], ticket, st),
+            CK(launch_lane(ls.nmax, ls.warps, ls.ring, ls.refill_k, ls.tail_k, ls.ctas, bc, list, escal_entries,
+                           &ctr->escal_count[c], &ctr->escal_claim[c], ticket, st),
                "launching per-lane kernel");
         } else if (c < 3) {
             const PoolShape &s = P.pool[c];
@@ -331,9 +331,9 @@ sbfs_status ensure_plan(sbfs_handle *h)
         s.ctas = per_sm * sms;
     }
     const int lane_defaults[2][4] = {
-        // warps, ring, refill_k (the autotuner's picks on B200 for uniform n = 8 and n = 12)
-        {8, 16, 16, 0},
-        {1, 64, 16, 0},
+        // warps, ring, refill_k, tail_k (the autotuner's picks on B200 for uniform n = 8 and n = 12)
+        {8, 16, 16, 8},
+        {1, 64, 16, 8},
     };
     for (int c = 0; c < 2; ++c) {
         LaneShape &ls = P.lane[c];
@@ -341,6 +341,7 @@ sbfs_status ensure_plan(sbfs_handle *h)
         ls.warps = h->cfg.lane_warps > 0 ? h->cfg.lane_warps : lane_defaults[c][0];
         ls.ring = h->cfg.lane_ring > 0 ? h->cfg.lane_ring : lane_defaults[c][1];
         ls.refill_k = h->cfg.lane_refill > 0 ? h->cfg.lane_refill : lane_defaults[c][2];
+        ls.tail_k = h->cfg.lane_tail > 0 ? std::min(h->cfg.lane_tail, 32) : h->cfg.lane_tail < 0 ? 0 : lane_defaults[c][3];
         if (lane_max_ctas_per_sm(ls.nmax, ls.warps, ls.ring) < 1) {
             ls.warps = lane_defaults[c][0];
             ls.ring = lane_defaults[c][1];

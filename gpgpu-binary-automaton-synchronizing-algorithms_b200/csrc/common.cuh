@@ -17,7 +17,6 @@ constexpr int32_t kLenInvalid = -2;   // malformed record (state >= n); host tur
 // Device error bits (one int per launch set, read back by the host).
 constexpr int kErrInvalid = 1;        // malformed automaton seen
 constexpr int kErrCapacity = 2;       // a queue or frontier exceeded its reserved space
-constexpr int kErrWait = 4;           // a bounded wait for another warp's store ran out
 
 // Everything a BFS kernel needs to know about the batch.
 struct Batch {
@@ -96,10 +95,12 @@ int pool_max_ctas_per_sm(const PoolShape &s);
 
 size_t lane_smem_bytes(int nmax, int warps, int ring);
 int lane_max_ctas_per_sm(int nmax, int warps, int ring);
-// escal_list must hold -1 in every entry the launch may append (count
-// entries); escal_count, escal_claim and drained start at 0.
-cudaError_t launch_lane(int nmax, int warps, int ring, int refill_k, int ctas, const Batch &b,
-                        int32_t *escal_list, unsigned long long *escal_count, unsigned long long *escal_claim,
-                        unsigned int *drained, unsigned long long *ticket, cudaStream_t st);
+// escal_list holds escal_capacity entries (>= the automata of the launch), all
+// -1; escal_count and escal_claim start at 0.
+// tail_k: once the batch is handed out, lanes of a warp with at most tail_k
+// lanes still searching give their automata to the whole-warp search (0 = off).
+cudaError_t launch_lane(int nmax, int warps, int ring, int refill_k, int tail_k, int ctas, const Batch &b,
+                        int32_t *escal_list, unsigned long long escal_capacity, unsigned long long *escal_count,
+                        unsigned long long *escal_claim, unsigned long long *ticket, cudaStream_t st);
 
 }  // namespace sbfs

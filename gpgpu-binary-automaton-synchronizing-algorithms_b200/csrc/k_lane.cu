@@ -25,15 +25,16 @@
 //
 // Two rare cases leave the per-lane search: a frontier wider than R, and (with
 // words) a word longer than 32 - NMAX letters.  Such an automaton is abandoned
-// and appended to the launch's escalation list.  A warp that has no lane work
-// left (no new automata, every lane idle) owns its whole shared-memory region
-// again and takes escalated automata from that list one at a time, solving
-// each with all 32 lanes: a level-synchronous search over a linear queue that
-// holds every subset at most once (2^n entries, so it cannot overflow), with
-// parent pointers for the word, the nibble table in registers read by warp
-// shuffles, and a linear bitmap updated with shared-memory atomics.  The last
-// warp to run out of lane work empties the list, so no escalated automaton is
-// left for another launch.
+// and appended to the launch's escalation list.  So is, once the batch is
+// handed out, the work of a warp with at most `tail_k` lanes still searching.
+// A warp that has no lane work left (no new automata, every lane idle) owns
+// its whole shared-memory region again and takes escalated automata from that
+// list one at a time, solving each with all 32 lanes: a level-synchronous
+// search over a linear queue that holds every subset at most once (2^n
+// entries, so it cannot overflow), with parent pointers for the word, the
+// nibble table in registers read by warp shuffles, and a linear bitmap updated
+// with shared-memory atomics.  Claims never wait (see claim_escalated): every
+// escalated automaton is solved in the launch that escalated it.
 //
 // Lanes that finish wait until `refill_k` lanes of the warp are idle; then the
 // warp writes their results and loads new automata for all of them in one
@@ -44,7 +45,7 @@
 namespace sbfs {
 namespace {
 
-constexpr int kActive = 0, kDone = 1, kEscalate = 2, kIdle = 3;
+constexpr int kActive = 0, kDone = 1, kEscalate = 2, kIdle = 3, kHeld = 4;
 
 __host__ __device__ constexpr int low_bit4(int v)
 {
@@ -85,30 +86,18 @@ __device__ __forceinline__ uint32_t table_entry(const uint8_t *rec, int lstride,
 }
 
 // Claims the next escalated automaton of the launch for a warp with no lane
-// work left, or returns -1 once there is none and none can come.  A claim is
-// one atomicAdd (never retried).  Its entry may not exist yet: it is appended
-// later by a warp still running lane work, or never, when every warp of the
-// launch has finished its lane work (each one fences its last append before it
-// counts itself in `drained`).  The writer bumps the count before it stores
-// the entry, so an entry is read until it is no longer -1.  All waits are
-// bounded (kErrWait on time-out).
-__device__ int64_t claim_escalated(const int32_t *list, const unsigned long long *count, unsigned long long *claim,
-                                   const unsigned int *drained, unsigned int warps, int *error)
+// work left, or returns -1.  A claim is one atomicAdd on the claim counter and
+// one atomicCAS on the claimed slot, raced against the slot's writer (which
+// stores with atomicCAS too): if the slot is still empty the claimer marks it
+// abandoned (-2) and stops, and the writer, finding it abandoned, keeps the
+// automaton and solves it itself once it runs out of lane work.  Nothing ever
+// waits for another warp.
+__device__ int64_t claim_escalated(int32_t *list, unsigned long long capacity, unsigned long long *claim)
 {
     const unsigned long long pos = atomicAdd(claim, 1ull);
-    for (int it = 0; it < (1 << 22); ++it) {
-        if (pos < *(volatile const unsigned long long *)count) {
-            const int32_t v = *(volatile const int32_t *)(list + pos);
-            if (v >= 0) return v;
-        } else if (*(volatile const unsigned int *)drained >= warps) {
-            __threadfence();
-            if (pos >= *(volatile const unsigned long long *)count) return -1;
-            continue;
-        }
-        __nanosleep(100);
-    }
-    atomicOr(error, kErrWait);
-    return -1;
+    if (pos >= capacity) return -1;
+    const int32_t prev = atomicCAS(list + pos, -1, -2);
+    return prev >= 0 ? (int64_t)prev : -1;
 }
 
 // One automaton (n <= NMAX) solved by the whole warp inside its region of
@@ -203,9 +192,9 @@ __device__ void warp_solve(const Batch &b, int64_t k, uint32_t *region, int lane
 }
 
 template <int NMAX, bool WORDS>
-__global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, int32_t *escal_list,
-                                              unsigned long long *escal_count, unsigned long long *escal_claim,
-                                              unsigned int *drained, unsigned long long *ticket)
+__global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, int tail_k, int32_t *escal_list,
+                                              unsigned long long escal_capacity, unsigned long long *escal_count,
+                                              unsigned long long *escal_claim, unsigned long long *ticket)
 {
     using G = LaneGeom<NMAX>;
     constexpr int BW = G::kBitmapWords;
@@ -234,6 +223,13 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
 
     while (true) {
         // ---- phase: finish waiting lanes, load new automata -----------------
+        // no new automata: once at most `tail_k` lanes still search, the warp
+        // hands their automata to the whole-warp search instead of finishing
+        // them at a few lanes' pace (the launch's tail)
+        if (!more && tail_k > 0) {
+            const unsigned active = __ballot_sync(kFull, state == kActive);
+            if (state == kActive && __popc(active) <= tail_k) state = kEscalate;
+        }
         const unsigned not_active = __ballot_sync(kFull, state != kActive);
         if (not_active == kFull ||
             (__popc(not_active) >= refill_k && (more || __any_sync(kFull, state == kDone || state == kEscalate)))) {
@@ -251,9 +247,14 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
                 const int leader = __ffs(esc) - 1;
                 if (lane == leader) pos = atomicAdd(escal_count, (unsigned long long)__popc(esc));
                 pos = __shfl_sync(kFull, pos, leader);
-                if (state == kEscalate) escal_list[pos + __popc(esc & ((1u << lane) - 1u))] = (int32_t)k;
+                if (state == kEscalate) {
+                    // a slot a drained warp already gave up on: solve this one ourselves later
+                    const int32_t prev =
+                        atomicCAS(escal_list + pos + __popc(esc & ((1u << lane) - 1u)), -1, (int32_t)k);
+                    state = prev == -1 ? kIdle : kHeld;
+                }
             }
-            if (state != kActive) state = kIdle;
+            if (state != kActive && state != kHeld) state = kIdle;
             const unsigned idle = __ballot_sync(kFull, state == kIdle);
             if (more && idle) {
                 unsigned long long got = 0;
@@ -333,16 +334,18 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
                 }
             }
             if (__ballot_sync(kFull, state == kActive) == 0u) {
+                // no lane is searching: the region is free for whole-warp searches,
+                // first of the automata this warp kept
+                for (unsigned held = __ballot_sync(kFull, state == kHeld); held; held &= held - 1u) {
+                    const int64_t e = __shfl_sync(kFull, k, __ffs(held) - 1);
+                    warp_solve<NMAX, WORDS>(b, e, base, lane, expanded);
+                }
+                if (state == kHeld) state = kIdle;
                 if (!more) {
-                    // no lane work left: the region is free for escalated automata
-                    if (lane == 0) {
-                        __threadfence();   // this warp's appends before its count
-                        atomicAdd(drained, 1u);
-                    }
-                    const unsigned int warps = gridDim.x * (blockDim.x >> 5);
+                    // no new automata either: solve escalated ones while any can be claimed
                     while (true) {
                         int64_t e = -1;
-                        if (lane == 0) e = claim_escalated(escal_list, escal_count, escal_claim, drained, warps, b.error);
+                        if (lane == 0) e = claim_escalated(escal_list, escal_capacity, escal_claim);
                         e = __shfl_sync(kFull, e, 0);
                         if (e < 0) break;
                         warp_solve<NMAX, WORDS>(b, e, base, lane, expanded);
@@ -424,9 +427,9 @@ size_t smem_for(int warps, int ring)
 }
 
 template <int NMAX, bool WORDS>
-cudaError_t launch_t(int warps, int ring, int refill_k, int ctas, const Batch &b, int32_t *escal_list,
-                     unsigned long long *escal_count, unsigned long long *escal_claim, unsigned int *drained,
-                     unsigned long long *ticket, cudaStream_t st)
+cudaError_t launch_t(int warps, int ring, int refill_k, int tail_k, int ctas, const Batch &b, int32_t *escal_list,
+                     unsigned long long escal_capacity, unsigned long long *escal_count,
+                     unsigned long long *escal_claim, unsigned long long *ticket, cudaStream_t st)
 {
     using G = LaneGeom<NMAX>;
     // the warp-cooperative search needs the bitmap and 2^NMAX queue entries in one region
@@ -434,8 +437,8 @@ cudaError_t launch_t(int warps, int ring, int refill_k, int ctas, const Batch &b
     const size_t smem = smem_for<NMAX>(warps, ring);
     cudaError_t e = cudaFuncSetAttribute(k_lane<NMAX, WORDS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_lane<NMAX, WORDS><<<ctas, warps * 32, smem, st>>>(b, ring, refill_k, escal_list, escal_count, escal_claim,
-                                                       drained, ticket);
+    k_lane<NMAX, WORDS><<<ctas, warps * 32, smem, st>>>(b, ring, refill_k, tail_k, escal_list, escal_capacity,
+                                                       escal_count, escal_claim, ticket);
     return cudaGetLastError();
 }
 
@@ -462,23 +465,24 @@ int lane_max_ctas_per_sm(int nmax, int warps, int ring)
     return blocks;
 }
 
-cudaError_t launch_lane(int nmax, int warps, int ring, int refill_k, int ctas, const Batch &b,
-                        int32_t *escal_list, unsigned long long *escal_count, unsigned long long *escal_claim,
-                        unsigned int *drained, unsigned long long *ticket, cudaStream_t st)
+cudaError_t launch_lane(int nmax, int warps, int ring, int refill_k, int tail_k, int ctas, const Batch &b,
+                        int32_t *escal_list, unsigned long long escal_capacity, unsigned long long *escal_count,
+                        unsigned long long *escal_claim, unsigned long long *ticket, cudaStream_t st)
 {
-    if ((ring & (ring - 1)) || ring < 8 || warps < 1 || warps > 8 || ctas < 1 || refill_k < 1 || refill_k > 32)
+    if ((ring & (ring - 1)) || ring < 8 || warps < 1 || warps > 8 || ctas < 1 || refill_k < 1 || refill_k > 32 ||
+        tail_k < 0 || tail_k > 32)
         return cudaErrorInvalidValue;
     const bool words = b.out_words != nullptr;
     if (nmax <= 8)
-        return words ? launch_t<8, true>(warps, ring, refill_k, ctas, b, escal_list, escal_count, escal_claim,
-                                         drained, ticket, st)
-                     : launch_t<8, false>(warps, ring, refill_k, ctas, b, escal_list, escal_count, escal_claim,
-                                          drained, ticket, st);
+        return words ? launch_t<8, true>(warps, ring, refill_k, tail_k, ctas, b, escal_list, escal_capacity,
+                                         escal_count, escal_claim, ticket, st)
+                     : launch_t<8, false>(warps, ring, refill_k, tail_k, ctas, b, escal_list, escal_capacity,
+                                          escal_count, escal_claim, ticket, st);
     if (nmax <= 12)
-        return words ? launch_t<12, true>(warps, ring, refill_k, ctas, b, escal_list, escal_count, escal_claim,
-                                          drained, ticket, st)
-                     : launch_t<12, false>(warps, ring, refill_k, ctas, b, escal_list, escal_count, escal_claim,
-                                           drained, ticket, st);
+        return words ? launch_t<12, true>(warps, ring, refill_k, tail_k, ctas, b, escal_list, escal_capacity,
+                                          escal_count, escal_claim, ticket, st)
+                     : launch_t<12, false>(warps, ring, refill_k, tail_k, ctas, b, escal_list, escal_capacity,
+                                           escal_count, escal_claim, ticket, st);
     return cudaErrorInvalidValue;
 }
 

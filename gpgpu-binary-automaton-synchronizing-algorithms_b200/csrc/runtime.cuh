@@ -24,10 +24,9 @@ struct DevCounters {
     unsigned long long first_violation;
     unsigned long long expanded;
     // per-lane kernels of classes 0 and 1: automata appended to the class's
-    // escalation list, claims on it, warps done with their lane work
+    // escalation list, and claims on it
     unsigned long long escal_count[2];
     unsigned long long escal_claim[2];
-    unsigned int lane_drained[2];
     int error;
     int pad;
     unsigned long long synchronizing;             // lengths >= 0 written by this job
@@ -57,6 +56,7 @@ struct LaneShape {
     int warps;      // warps per CTA
     int ring;       // on-chip frontier ring entries per lane (power of two)
     int refill_k;   // idle lanes that trigger a refill pass
+    int tail_k;     // at most this many searching lanes after the last refill: hand them to the warp
     int ctas;       // grid size (persistent)
 };
 

@@ -80,7 +80,7 @@ std::string device_key(sbfs_handle *h)
     cudaDeviceProp p;
     cudaGetDeviceProperties(&p, h->device);
     char buf[320];
-    std::snprintf(buf, sizeof buf, "%s|sm%d|abi%d|v5", p.name, h->sm_count, SBFS_ABI_VERSION);
+    std::snprintf(buf, sizeof buf, "%s|sm%d|abi%d|v6", p.name, h->sm_count, SBFS_ABI_VERSION);
     for (char *c = buf; *c; ++c)
         if (*c == ' ') *c = '_';
     return buf;
@@ -90,11 +90,12 @@ std::string encode(const Plan &P)
 {
     char buf[512];
     std::snprintf(buf, sizeof buf,
-                  "c0=%d,%d,%d,%d,%d,%d,%d c1=%d,%d,%d,%d,%d,%d,%d c2=%d,%d,%d c3=%d,%d",
-                  P.use_pool[0], P.lane[0].warps, P.lane[0].ring, P.lane[0].refill_k, P.pool[0].slots, P.pool[0].warps,
-                  P.pool[0].queue_smem, P.use_pool[1], P.lane[1].warps, P.lane[1].ring, P.lane[1].refill_k,
-                  P.pool[1].slots, P.pool[1].warps, P.pool[1].queue_smem, P.pool[2].slots, P.pool[2].warps,
-                  P.pool[2].queue_smem, P.class3_level, P.cta.threads);
+                  "c0=%d,%d,%d,%d,%d,%d,%d,%d c1=%d,%d,%d,%d,%d,%d,%d,%d c2=%d,%d,%d c3=%d,%d",
+                  P.use_pool[0], P.lane[0].warps, P.lane[0].ring, P.lane[0].refill_k, P.lane[0].tail_k,
+                  P.pool[0].slots, P.pool[0].warps, P.pool[0].queue_smem, P.use_pool[1], P.lane[1].warps,
+                  P.lane[1].ring, P.lane[1].refill_k, P.lane[1].tail_k, P.pool[1].slots, P.pool[1].warps,
+                  P.pool[1].queue_smem, P.pool[2].slots, P.pool[2].warps, P.pool[2].queue_smem, P.class3_level,
+                  P.cta.threads);
     return buf;
 }
 
@@ -102,12 +103,12 @@ bool decode(const char *s, Plan &P)
 {
     Plan Q = P;
     const int got = std::sscanf(
-        s, "c0=%d,%d,%d,%d,%d,%d,%d c1=%d,%d,%d,%d,%d,%d,%d c2=%d,%d,%d c3=%d,%d", &Q.use_pool[0], &Q.lane[0].warps,
-        &Q.lane[0].ring, &Q.lane[0].refill_k, &Q.pool[0].slots, &Q.pool[0].warps, &Q.pool[0].queue_smem,
-        &Q.use_pool[1], &Q.lane[1].warps, &Q.lane[1].ring, &Q.lane[1].refill_k, &Q.pool[1].slots, &Q.pool[1].warps,
-        &Q.pool[1].queue_smem, &Q.pool[2].slots, &Q.pool[2].warps, &Q.pool[2].queue_smem, &Q.class3_level,
-        &Q.cta.threads);
-    if (got != 19) return false;
+        s, "c0=%d,%d,%d,%d,%d,%d,%d,%d c1=%d,%d,%d,%d,%d,%d,%d,%d c2=%d,%d,%d c3=%d,%d", &Q.use_pool[0],
+        &Q.lane[0].warps, &Q.lane[0].ring, &Q.lane[0].refill_k, &Q.lane[0].tail_k, &Q.pool[0].slots,
+        &Q.pool[0].warps, &Q.pool[0].queue_smem, &Q.use_pool[1], &Q.lane[1].warps, &Q.lane[1].ring,
+        &Q.lane[1].refill_k, &Q.lane[1].tail_k, &Q.pool[1].slots, &Q.pool[1].warps, &Q.pool[1].queue_smem,
+        &Q.pool[2].slots, &Q.pool[2].warps, &Q.pool[2].queue_smem, &Q.class3_level, &Q.cta.threads);
+    if (got != 21) return false;
     P = Q;
     return true;
 }
@@ -191,23 +192,25 @@ cudaError_t plan_autotune(sbfs_handle *h, Plan &plan)
         const int warps_c[2][3] = {{2, 4, 8}, {1, 2, 0}};
         for (int w : warps_c[c])
             for (int ring : {16, 32, 64})
-                for (int rk : {8, 16}) {
-                    if (!w) continue;
-                    Plan t = P;
-                    t.use_pool[c] = 0;
-                    t.lane[c].warps = w;
-                    t.lane[c].ring = ring;
-                    t.lane[c].refill_k = rk;
-                    const int per = lane_max_ctas_per_sm(n, w, ring);
-                    if (per < 1) continue;
-                    t.lane[c].ctas = per * h->sm_count;
-                    h->plan = t;
-                    const double ms = time_plan(b, n, count);
-                    if (ms < best_ms) {
-                        best_ms = ms;
-                        best = t;
+                for (int rk : {8, 16})
+                    for (int tk : {0, 8, 16}) {
+                        if (!w) continue;
+                        Plan t = P;
+                        t.use_pool[c] = 0;
+                        t.lane[c].warps = w;
+                        t.lane[c].ring = ring;
+                        t.lane[c].refill_k = rk;
+                        t.lane[c].tail_k = tk;
+                        const int per = lane_max_ctas_per_sm(n, w, ring);
+                        if (per < 1) continue;
+                        t.lane[c].ctas = per * h->sm_count;
+                        h->plan = t;
+                        const double ms = time_plan(b, n, count);
+                        if (ms < best_ms) {
+                            best_ms = ms;
+                            best = t;
+                        }
                     }
-                }
         for (int S : {4, 8, 16})
             for (int W : {1, 2, 4})
                 for (int Q : {64, 128}) {

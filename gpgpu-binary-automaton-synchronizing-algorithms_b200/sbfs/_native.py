@@ -55,6 +55,7 @@ class Config(ctypes.Structure):
         ("lane_ring", ctypes.c_int32),
         ("lane_refill", ctypes.c_int32),
         ("lane_warps", ctypes.c_int32),
+        ("lane_tail", ctypes.c_int32),
         ("streams", ctypes.c_int32),
         ("level_arena_bytes", ctypes.c_int64),
         ("tune_cache", ctypes.c_char_p),

@@ -39,7 +39,7 @@ class Engine:
     def __init__(self, device: int = -1, slack: int = 0, autotune: bool = False, use_graph: bool = False,
                  slots_per_warp: int = 0, warps_per_cta: int = 0, queue_smem: int = 0, chunk: int = 0,
                  small_kernel: int = 0, lane_ring: int = 0, lane_refill: int = 0, lane_warps: int = 0,
-                 streams: int = 0,
+                 lane_tail: int = 0, streams: int = 0,
                  level_arena_bytes: int = 0, tune_cache: Optional[str] = None):
         self.lib = _native.load()
         cfg = _native.Config()
@@ -55,6 +55,7 @@ class Engine:
         cfg.small_kernel = small_kernel
         cfg.lane_ring = lane_ring
         cfg.lane_refill = lane_refill
+        cfg.lane_tail = lane_tail
         cfg.lane_warps = lane_warps
         cfg.streams = streams
         cfg.level_arena_bytes = level_arena_bytes

@@ -86,6 +86,9 @@ typedef struct sbfs_config {
     int32_t lane_ring;         /* per-lane kernel: on-chip frontier entries (power of 2); 0 = auto */
     int32_t lane_refill;       /* per-lane kernel: idle lanes that trigger a refill; 0 = auto */
     int32_t lane_warps;        /* per-lane kernel: warps per CTA; 0 = auto              */
+    int32_t lane_tail;         /* per-lane kernel: after the last automaton is handed out, a warp with at most
+                                  this many lanes still searching gives them to the whole-warp search;
+                                  0 = auto, -1 = never                                     */
     int32_t streams;           /* streams the host path rotates chunks over; 0 = 4      */
     int64_t level_arena_bytes; /* HBM budget of the n > 20 level slots; 0 = half of free memory, <= 64 GiB */
     const char *tune_cache;    /* autotuner cache file, or NULL for in-memory only      */
