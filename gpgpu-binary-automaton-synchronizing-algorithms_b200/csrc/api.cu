@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <thread>
 
 #include "runtime.cuh"
 
@@ -57,7 +58,8 @@ cudaError_t HostBuf::reserve(size_t want)
     if (want <= bytes && ptr) return cudaSuccess;
     release();
     size_t sz = std::max<size_t>(want, 256);
-    cudaError_t e = cudaHostAlloc(&ptr, sz, cudaHostAllocDefault);
+    // mapped, so kernels may store into it (the streamed host path's chunk flags)
+    cudaError_t e = cudaHostAlloc(&ptr, sz, cudaHostAllocMapped);
     if (e != cudaSuccess) {
         ptr = nullptr;
         cudaGetLastError();
@@ -269,7 +271,7 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
             int32_t *list = L.escal.as<int32_t>() + (size_t)c * escal_entries;
             CK(cudaMemsetAsync(list, 0xFF, escal_entries * sizeof(int32_t), st), "resetting escalation list");
             CK(launch_lane(ls.nmax, ls.warps, ls.ring, ls.refill_k, ls.tail_k, ls.ctas, bc, list, escal_entries,
-                           &ctr->escal_count[c], &ctr->escal_claim[c], ticket, st),
+                           &ctr->escal_count[c], &ctr->escal_claim[c], ticket, LaneStream{}, st),
                "launching per-lane kernel");
         } else if (c < 3) {
             const PoolShape &s = P.pool[c];
@@ -495,6 +497,222 @@ std::string graph_key(const void *a, const void *b, const void *c, const void *d
     return buf;
 }
 
+// Streamed host path for a uniform batch of n <= 12 on the per-lane kernel:
+// one kernel launch per job instead of one per chunk (each launch pays the
+// BFS's longest tail), with the copies of both directions overlapping it.
+//  - copy_in: records chunk by chunk, each followed by its chunk_ready flag;
+//    the kernel waits (bounded) only for a chunk its ticket has reached;
+//  - the kernel counts lane outcomes per chunk and the warp that completes a
+//    chunk sets the chunk's flag in mapped host memory;
+//  - this thread polls those flags and copies each finished chunk's lengths
+//    and words out on copy_out while the kernel still runs;
+//  - automata solved by the whole-warp search finish late: they are also
+//    written to a compact array (by escalation slot), copied back at the end
+//    and patched into the host results.
+constexpr int64_t kStreamChunk = 1 << 17;   // x 2n bytes: whole 128-byte lines
+constexpr int64_t kStreamJob = 1 << 24;     // automata per kernel launch
+
+bool stream_eligible(sbfs_handle *h, const uint8_t *ns, int32_t n_uniform, int64_t count, bool plain)
+{
+    if (plain || ns || h->cfg.chunk != 0 || count < 2 * kStreamChunk) return false;
+    const int c = class_of_n(n_uniform);
+    return c < 2 && !h->plan.use_pool[c];
+}
+
+struct StreamOut {
+    int64_t expanded = 0, escalated = 0, synchronizing = 0, first_violation = -1;
+    int error = 0;
+    double kernel_ms = 0;
+    int launches = 0;
+};
+
+sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstride, int32_t n, int64_t cnt,
+                               int32_t *out_len, uint64_t *out_words, int32_t ws, bool pin_in, bool pin_out,
+                               StreamOut &o)
+{
+    Lane &L = h->lanes[0];
+    Streamer &S = h->streamer;
+    const size_t rec = 2 * (size_t)lstride;
+    const int64_t nch = (cnt + kStreamChunk - 1) / kStreamChunk;
+    const int c = class_of_n(n);
+    const LaneShape &ls = h->plan.lane[c];
+    CK(L.maps.reserve(cnt * rec), "allocating records");
+    if (out_len) CK(L.len.reserve(cnt * sizeof(int32_t)), "allocating lengths");
+    if (out_words) CK(L.words.reserve((size_t)cnt * ws * sizeof(uint64_t)), "allocating words");
+    CK(L.counters.reserve(sizeof(DevCounters)), "allocating counters");
+    CK(L.h_counters.reserve(sizeof(DevCounters)), "allocating pinned counters");
+    CK(L.escal.reserve((size_t)cnt * sizeof(int32_t)), "allocating escalation list");
+    CK(S.flags.reserve(2 * (size_t)nch * sizeof(unsigned int)), "allocating chunk flags");
+    CK(S.escal_out.reserve((size_t)cnt * sizeof(EscalResult)), "allocating escalated results");
+    CK(S.h_flags.reserve(3 * (size_t)nch * sizeof(unsigned int)), "allocating host chunk flags");
+    unsigned int *hf = S.h_flags.as<unsigned int>();   // host_flag | zeros | ones
+    for (int64_t i = 0; i < nch; ++i) {
+        hf[i] = 0u;
+        hf[nch + i] = 0u;
+        hf[2 * nch + i] = 1u;
+    }
+    unsigned int *d_host_flag = nullptr;
+    CK(cudaHostGetDevicePointer((void **)&d_host_flag, hf, 0), "mapping host chunk flags");
+    unsigned int *ready = S.flags.as<unsigned int>(), *done = ready + nch;
+    const uint8_t *src = maps;
+    if (!pin_in) {
+        CK(L.h_maps.reserve(cnt * rec), "allocating pinned staging");
+        std::memcpy(L.h_maps.ptr, maps, cnt * rec);
+        src = L.h_maps.as<uint8_t>();
+    }
+    int32_t *dst_len = out_len;
+    uint64_t *dst_words = out_words;
+    if (!pin_out) {
+        if (out_len) {
+            CK(L.h_len.reserve(cnt * sizeof(int32_t)), "allocating pinned staging");
+            dst_len = L.h_len.as<int32_t>();
+        }
+        if (out_words) {
+            CK(L.h_words.reserve((size_t)cnt * ws * sizeof(uint64_t)), "allocating pinned staging");
+            dst_words = L.h_words.as<uint64_t>();
+        }
+    }
+    // flags through the copy engine only: a memset could need an SM that the
+    // running kernel holds
+    CK(cudaMemcpyAsync(ready, hf + nch, nch * sizeof(unsigned int), cudaMemcpyHostToDevice, h->copy_in),
+       "clearing chunk flags");
+    auto copy_chunk_in = [&](int64_t ci) -> sbfs_status {
+        const int64_t a = ci * kStreamChunk, m = std::min(kStreamChunk, cnt - a);
+        CK(cudaMemcpyAsync(L.maps.as<uint8_t>() + a * rec, src + a * rec, m * rec, cudaMemcpyHostToDevice,
+                           h->copy_in),
+           "copying records");
+        CK(cudaMemcpyAsync(ready + ci, hf + 2 * nch + ci, sizeof(unsigned int), cudaMemcpyHostToDevice, h->copy_in),
+           "setting a chunk flag");
+        return SBFS_OK;
+    };
+    sbfs_status st = copy_chunk_in(0);
+    if (st) return st;
+    CK(cudaEventRecord(S.ev_in0, h->copy_in), "recording event");
+    // the kernel, behind chunk 0
+    CK(cudaStreamWaitEvent(L.stream, S.ev_in0, 0), "ordering streams");
+    CK(cudaMemsetAsync(L.counters.ptr, 0, sizeof(DevCounters), L.stream), "resetting counters");
+    CK(cudaMemsetAsync(&L.counters.as<DevCounters>()->first_violation, 0xFF, sizeof(unsigned long long), L.stream),
+       "resetting counters");
+    CK(cudaMemsetAsync(L.escal.ptr, 0xFF, (size_t)cnt * sizeof(int32_t), L.stream), "resetting escalation list");
+    CK(cudaMemsetAsync(done, 0, nch * sizeof(unsigned int), L.stream), "resetting chunk counts");
+    DevCounters *ctr = L.counters.as<DevCounters>();
+    Batch b{};
+    b.maps = L.maps.as<uint8_t>();
+    b.lstride = lstride;
+    b.n_uniform = n;
+    b.count = cnt;
+    b.out_len = out_len ? L.len.as<int32_t>() : nullptr;
+    b.out_words = out_words ? L.words.as<uint64_t>() : nullptr;
+    b.word_stride = out_words ? ws : 0;
+    b.slack = h->cfg.slack;
+    b.first_violation = &ctr->first_violation;
+    b.expanded = &ctr->expanded;
+    b.error = &ctr->error;
+    LaneStream lsd{ready, done, d_host_flag, kStreamChunk, S.escal_out.as<EscalResult>()};
+    CK(cudaEventRecord(L.ev_k0, L.stream), "recording event");
+    CK(launch_lane(ls.nmax, ls.warps, ls.ring, ls.refill_k, ls.tail_k, ls.ctas, b, L.escal.as<int32_t>(),
+                   (unsigned long long)cnt, &ctr->escal_count[c], &ctr->escal_claim[c], &ctr->ticket[c], lsd,
+                   L.stream),
+       "launching per-lane kernel");
+    CK(cudaEventRecord(L.ev_k1, L.stream), "recording event");
+    o.launches += 1;
+    if (out_len) {
+        CK(launch_count_sync(b.out_len, cnt, &ctr->synchronizing, h->sm_count, L.stream), "launching result count");
+        o.launches += 1;
+    }
+    CK(cudaMemcpyAsync(L.h_counters.ptr, L.counters.ptr, sizeof(DevCounters), cudaMemcpyDeviceToHost, L.stream),
+       "copying counters");
+    CK(cudaEventRecord(S.ev_kdone, L.stream), "recording event");
+    for (int64_t ci = 1; ci < nch; ++ci)
+        if ((st = copy_chunk_in(ci))) return st;
+    // results out, chunk by chunk, as the kernel finishes them
+    auto copy_chunk_out = [&](int64_t ci) -> sbfs_status {
+        const int64_t a = ci * kStreamChunk, m = std::min(kStreamChunk, cnt - a);
+        if (out_len)
+            CK(cudaMemcpyAsync(dst_len + a, L.len.as<int32_t>() + a, m * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                               S.copy_out),
+               "copying lengths");
+        if (out_words)
+            CK(cudaMemcpyAsync(dst_words + (size_t)a * ws, L.words.as<uint64_t>() + (size_t)a * ws,
+                               (size_t)m * ws * sizeof(uint64_t), cudaMemcpyDeviceToHost, S.copy_out),
+               "copying words");
+        return SBFS_OK;
+    };
+    const auto t_start = std::chrono::steady_clock::now();
+    int64_t next = 0;
+    while (next < nch) {
+        if (*(volatile unsigned int *)(hf + next)) {
+            if ((st = copy_chunk_out(next))) return st;
+            ++next;
+            continue;
+        }
+        const cudaError_t q = cudaEventQuery(S.ev_kdone);
+        if (q == cudaSuccess) break;
+        if (q != cudaErrorNotReady) CK(q, "waiting for the kernel");
+        if (std::chrono::steady_clock::now() - t_start > std::chrono::seconds(600))
+            return fail(h, SBFS_ETIMEOUT, "streamed solve: no progress for 600 s");
+        std::this_thread::yield();
+    }
+    CK(cudaEventSynchronize(S.ev_kdone), "waiting for the kernel");
+    for (; next < nch; ++next)
+        if ((st = copy_chunk_out(next))) return st;
+    // escalated automata finish after their chunk may have been copied: store
+    // their results into the host output from the device, behind the copies
+    int32_t *map_len = nullptr;
+    uint64_t *map_words = nullptr;
+    bool mapped = true;
+    if (dst_len && cudaHostGetDevicePointer((void **)&map_len, dst_len, 0) != cudaSuccess) mapped = false;
+    if (dst_words && cudaHostGetDevicePointer((void **)&map_words, dst_words, 0) != cudaSuccess) mapped = false;
+    cudaGetLastError();
+    const DevCounters *hc = L.h_counters.as<DevCounters>();
+    const int64_t esc = (int64_t)hc->escal_count[c];
+    if (esc > 0 && (out_len || out_words)) {
+        if (mapped) {
+            CK(launch_escal_patch(S.escal_out.as<EscalResult>(), &ctr->escal_count[c], map_len, map_words, ws,
+                                  h->sm_count, S.copy_out),
+               "launching result patch");
+            o.launches += 1;
+        } else {
+            CK(S.h_escal.reserve((size_t)esc * sizeof(EscalResult)), "allocating escalated results");
+            CK(cudaMemcpyAsync(S.h_escal.ptr, S.escal_out.ptr, (size_t)esc * sizeof(EscalResult),
+                               cudaMemcpyDeviceToHost, S.copy_out),
+               "copying escalated results");
+        }
+    }
+    CK(cudaStreamSynchronize(S.copy_out), "copying results");
+    if (esc > 0 && (out_len || out_words) && !mapped) {
+        const EscalResult *r = S.h_escal.as<EscalResult>();
+        for (int64_t i = 0; i < esc; ++i) {
+            if (i + 16 < esc) {   // the stores miss the cache: keep several in flight
+                if (dst_len) __builtin_prefetch(dst_len + r[i + 16].k, 1);
+                if (dst_words) __builtin_prefetch(dst_words + (size_t)r[i + 16].k * ws, 1);
+            }
+            const int64_t k = r[i].k;
+            if (k < 0 || k >= cnt) return fail(h, SBFS_ECUDA, "streamed solve: corrupt escalated result");
+            if (dst_len) dst_len[k] = r[i].len;
+            if (dst_words) {
+                uint64_t *w = dst_words + (size_t)k * ws;
+                w[0] = r[i].word[0];
+                if (ws > 1) w[1] = r[i].word[1];
+                for (int j = 2; j < ws; ++j) w[j] = 0ull;
+            }
+        }
+    }
+    if (!pin_out) {
+        if (out_len) std::memcpy(out_len, dst_len, cnt * sizeof(int32_t));
+        if (out_words) std::memcpy(out_words, dst_words, (size_t)cnt * ws * sizeof(uint64_t));
+    }
+    o.expanded += (int64_t)hc->expanded;
+    o.escalated += esc;
+    o.synchronizing += (int64_t)hc->synchronizing;
+    o.error |= hc->error;
+    if (hc->first_violation != ULLONG_MAX && o.first_violation < 0) o.first_violation = (int64_t)hc->first_violation;
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, L.ev_k0, L.ev_k1) == cudaSuccess) o.kernel_ms += ms;
+    cudaGetLastError();
+    return SBFS_OK;
+}
+
 sbfs_status solve_host(sbfs_handle *h, const uint8_t *maps, int32_t lstride, const uint8_t *ns,
                        int32_t n_uniform, int64_t count, int32_t *out_len, uint64_t *out_words,
                        int32_t word_stride, int64_t *out_first_violation, sbfs_stats *stats, bool plain)
@@ -512,6 +730,39 @@ sbfs_status solve_host(sbfs_handle *h, const uint8_t *maps, int32_t lstride, con
     if ((s = ensure_plan(h))) return s;
 
     if (h->device_pending) CK(cudaEventSynchronize(h->ev_device), "waiting for device work");
+    if (stream_eligible(h, ns, n_uniform, count, plain)) {
+        const bool s_pin_in = is_pinned(maps), s_pin_out = is_pinned(out_len) && is_pinned(out_words);
+        const int32_t ws = out_words ? word_stride : 0;
+        StreamOut so;
+        for (int64_t begin = 0; begin < count; begin += kStreamJob) {
+            const int64_t cnt = std::min(kStreamJob, count - begin);
+            const int64_t fv_before = so.first_violation;
+            so.first_violation = -1;
+            s = solve_streamed_job(h, maps + (size_t)begin * 2 * lstride, lstride, n_uniform, cnt,
+                                   out_len ? out_len + begin : nullptr,
+                                   out_words ? out_words + (size_t)begin * ws : nullptr, ws, s_pin_in, s_pin_out, so);
+            if (s) return s;
+            so.first_violation =
+                fv_before >= 0 ? fv_before : (so.first_violation >= 0 ? begin + so.first_violation : -1);
+        }
+        if (out_first_violation) *out_first_violation = so.first_violation;
+        if (stats) {
+            stats->automata = count;
+            stats->expanded = so.expanded;
+            stats->synchronizing = so.synchronizing;
+            stats->h2d_bytes = count * 2 * (int64_t)lstride;
+            stats->d2h_bytes = (out_len ? count * 4 : 0) + (out_words ? count * (int64_t)ws * 8 : 0);
+            stats->launches = so.launches;
+            stats->classes = 1;
+            stats->kernel_ms = so.kernel_ms;
+            stats->escalated = so.escalated;
+            stats->total_ms =
+                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        }
+        if (so.error & kErrInvalid) return fail(h, SBFS_EINVAL, "malformed automaton: a state index >= n");
+        if (so.error) return fail(h, SBFS_ETIMEOUT, "a device-side bounded wait ran out");
+        return SBFS_OK;
+    }
     const int64_t chunk = plain ? std::max<int64_t>(count, 1)
                                 : (h->cfg.chunk > 0 ? h->cfg.chunk : kDefaultChunk);
     const bool pin_in = is_pinned(maps) && is_pinned(ns);
@@ -747,7 +998,10 @@ sbfs_status sbfs_create(const sbfs_config *cfg, sbfs_handle **out)
     h->lanes.resize(c.streams > 0 ? std::min(c.streams, 16) : kDefaultLanes);
     if ((e = cudaEventCreateWithFlags(&h->ev_device, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreate(&h->ev_dk0)) != cudaSuccess || (e = cudaEventCreate(&h->ev_dk1)) != cudaSuccess ||
-        (e = cudaStreamCreateWithFlags(&h->copy_in, cudaStreamNonBlocking)) != cudaSuccess) {
+        (e = cudaStreamCreateWithFlags(&h->copy_in, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&h->streamer.copy_out, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&h->streamer.ev_in0, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&h->streamer.ev_kdone, cudaEventDisableTiming)) != cudaSuccess) {
         sbfs_destroy(h);
         return cuda_fail(nullptr, e, "creating events");
     }
@@ -795,6 +1049,19 @@ sbfs_status sbfs_destroy(sbfs_handle *h)
     if (h->copy_in) {
         cudaStreamSynchronize(h->copy_in);
         cudaStreamDestroy(h->copy_in);
+    }
+    {
+        Streamer &S = h->streamer;
+        if (S.copy_out) {
+            cudaStreamSynchronize(S.copy_out);
+            cudaStreamDestroy(S.copy_out);
+        }
+        if (S.ev_in0) cudaEventDestroy(S.ev_in0);
+        if (S.ev_kdone) cudaEventDestroy(S.ev_kdone);
+        S.flags.release();
+        S.escal_out.release();
+        S.h_flags.release();
+        S.h_escal.release();
     }
     if (h->ev_device) cudaEventDestroy(h->ev_device);
     if (h->ev_dk0) cudaEventDestroy(h->ev_dk0);

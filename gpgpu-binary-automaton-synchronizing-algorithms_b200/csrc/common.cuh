@@ -17,6 +17,7 @@ constexpr int32_t kLenInvalid = -2;   // malformed record (state >= n); host tur
 // Device error bits (one int per launch set, read back by the host).
 constexpr int kErrInvalid = 1;        // malformed automaton seen
 constexpr int kErrCapacity = 2;       // a queue or frontier exceeded its reserved space
+constexpr int kErrWait = 4;           // a bounded wait for streamed input ran out
 
 // Everything a BFS kernel needs to know about the batch.
 struct Batch {
@@ -95,12 +96,35 @@ int pool_max_ctas_per_sm(const PoolShape &s);
 
 size_t lane_smem_bytes(int nmax, int warps, int ring);
 int lane_max_ctas_per_sm(int nmax, int warps, int ring);
+// Streaming form of the per-lane kernel (host path, uniform batch in
+// order): records arrive chunk by chunk while the kernel runs, and results
+// leave chunk by chunk.  All pointers null = everything resident, no tracking.
+struct EscalResult {
+    int64_t k;          // automaton
+    int32_t len;
+    int32_t pad;
+    uint64_t word[2];   // n <= 12: at most 121 letters
+};
+struct LaneStream {
+    const unsigned int *chunk_ready;   // nonzero once chunk c's records are on the device
+    unsigned int *chunk_done;          // lane outcomes recorded per chunk (starts at 0)
+    unsigned int *host_flag;           // mapped host memory: 1 once chunk c's outcomes are all written
+    int64_t chunk;                     // automata per chunk (records of a chunk fill whole 128-byte lines)
+    EscalResult *escal_out;            // by escalation slot: results the whole-warp search writes
+};
+
+// Stores the first *count escalated results into device-accessible (e.g.
+// mapped host) len / words (either may be null).
+cudaError_t launch_escal_patch(const EscalResult *r, const unsigned long long *count, int32_t *len, uint64_t *words,
+                               int ws, int sm_count, cudaStream_t st);
+
 // escal_list holds escal_capacity entries (>= the automata of the launch), all
 // -1; escal_count and escal_claim start at 0.
 // tail_k: once the batch is handed out, lanes of a warp with at most tail_k
 // lanes still searching give their automata to the whole-warp search (0 = off).
 cudaError_t launch_lane(int nmax, int warps, int ring, int refill_k, int tail_k, int ctas, const Batch &b,
                         int32_t *escal_list, unsigned long long escal_capacity, unsigned long long *escal_count,
-                        unsigned long long *escal_claim, unsigned long long *ticket, cudaStream_t st);
+                        unsigned long long *escal_claim, unsigned long long *ticket, const LaneStream &ls,
+                        cudaStream_t st);
 
 }  // namespace sbfs

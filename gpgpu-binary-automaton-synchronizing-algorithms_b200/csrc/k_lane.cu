@@ -92,19 +92,34 @@ __device__ __forceinline__ uint32_t table_entry(const uint8_t *rec, int lstride,
 // abandoned (-2) and stops, and the writer, finding it abandoned, keeps the
 // automaton and solves it itself once it runs out of lane work.  Nothing ever
 // waits for another warp.
-__device__ int64_t claim_escalated(int32_t *list, unsigned long long capacity, unsigned long long *claim)
+__device__ int64_t claim_escalated(int32_t *list, unsigned long long capacity, unsigned long long *claim,
+                                   unsigned long long &slot)
 {
-    const unsigned long long pos = atomicAdd(claim, 1ull);
-    if (pos >= capacity) return -1;
-    const int32_t prev = atomicCAS(list + pos, -1, -2);
+    slot = atomicAdd(claim, 1ull);
+    if (slot >= capacity) return -1;
+    const int32_t prev = atomicCAS(list + slot, -1, -2);
     return prev >= 0 ? (int64_t)prev : -1;
+}
+
+// Waits (bounded) until the streamed records of chunk c are on the device.
+__device__ bool wait_chunk(const unsigned int *ready, int64_t c)
+{
+    for (int it = 0; it < (1 << 24); ++it) {
+        if (*(volatile const unsigned int *)(ready + c)) {
+            __threadfence();
+            return true;
+        }
+        __nanosleep(200);
+    }
+    return false;
 }
 
 // One automaton (n <= NMAX) solved by the whole warp inside its region of
 // `region_words` shared words (>= 2^NMAX / 32 + 2^NMAX).  Queue entry:
 // subset | parent index << NMAX | letter << 2*NMAX (letter 1 = b).
-template <int NMAX, bool WORDS>
-__device__ void warp_solve(const Batch &b, int64_t k, uint32_t *region, int lane, unsigned long long &expanded)
+template <int NMAX, bool WORDS, bool STREAM>
+__device__ void warp_solve(const Batch &b, int64_t k, uint32_t *region, int lane, unsigned long long &expanded,
+                           const LaneStream &ls, unsigned long long slot)
 {
     using G = LaneGeom<NMAX>;
     constexpr int BW = G::kBitmapWords;
@@ -166,9 +181,9 @@ __device__ void warp_solve(const Batch &b, int64_t k, uint32_t *region, int lane
     }
     if (lane == 0) {
         record_result(b, k, n, len);
+        uint64_t w0 = 0, w1 = 0;
         if (WORDS) {
             // letters from the root: entry at depth d + 1 holds letter d
-            uint64_t w0 = 0, w1 = 0;
             if (len > 0) {
                 auto set = [&](uint32_t d) {
                     if (d < 64) w0 |= 1ull << d;
@@ -187,14 +202,25 @@ __device__ void warp_solve(const Batch &b, int64_t k, uint32_t *region, int lane
             if (b.word_stride > 1) w[1] = w1;
             for (int c = 2; c < b.word_stride; ++c) w[c] = 0ull;
         }
+        if (STREAM && ls.escal_out) {
+            // streamed batches: the host patches escalated automata from here
+            EscalResult r;
+            r.k = k;
+            r.len = len;
+            r.pad = 0;
+            r.word[0] = w0;
+            r.word[1] = w1;
+            ls.escal_out[slot] = r;
+        }
     }
     __syncwarp();
 }
 
-template <int NMAX, bool WORDS>
+template <int NMAX, bool WORDS, bool STREAM>
 __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, int tail_k, int32_t *escal_list,
                                               unsigned long long escal_capacity, unsigned long long *escal_count,
-                                              unsigned long long *escal_claim, unsigned long long *ticket)
+                                              unsigned long long *escal_claim, unsigned long long *ticket,
+                                              LaneStream ls)
 {
     using G = LaneGeom<NMAX>;
     constexpr int BW = G::kBitmapWords;
@@ -220,6 +246,8 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
     uint32_t res_word = 0;
     bool more = true;
     unsigned long long expanded = 0;
+    unsigned long long hslot = 0;   // escalation slot of a held automaton
+    int64_t ready_upto = -1;        // streamed chunks known to be on the device
 
     while (true) {
         // ---- phase: finish waiting lanes, load new automata -----------------
@@ -233,6 +261,7 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
         const unsigned not_active = __ballot_sync(kFull, state != kActive);
         if (not_active == kFull ||
             (__popc(not_active) >= refill_k && (more || __any_sync(kFull, state == kDone || state == kEscalate)))) {
+            const bool outcome = state == kDone || state == kEscalate;
             if (state == kDone) {
                 record_result(b, k, n, res_len);
                 if (WORDS) {
@@ -249,9 +278,29 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
                 pos = __shfl_sync(kFull, pos, leader);
                 if (state == kEscalate) {
                     // a slot a drained warp already gave up on: solve this one ourselves later
-                    const int32_t prev =
-                        atomicCAS(escal_list + pos + __popc(esc & ((1u << lane) - 1u)), -1, (int32_t)k);
+                    const unsigned long long slot = pos + __popc(esc & ((1u << lane) - 1u));
+                    const int32_t prev = atomicCAS(escal_list + slot, -1, (int32_t)k);
                     state = prev == -1 ? kIdle : kHeld;
+                    hslot = slot;
+                }
+            }
+            if (STREAM) {
+                // streamed batch: count outcomes per chunk; whoever completes a
+                // chunk tells the host its lengths and words can be copied out
+                const unsigned om = __ballot_sync(kFull, outcome);
+                if (outcome) {
+                    __threadfence();   // this lane's results before its count
+                    const int64_t c = k / ls.chunk;
+                    const unsigned grp = __match_any_sync(om, (unsigned long long)c);
+                    if (lane == __ffs(grp) - 1) {
+                        const unsigned add = (unsigned)__popc(grp);
+                        const unsigned old = atomicAdd(ls.chunk_done + c, add);
+                        const int64_t size = min(ls.chunk, count - c * ls.chunk);
+                        if ((int64_t)(old + add) == size) {
+                            __threadfence_system();
+                            *(volatile unsigned int *)(ls.host_flag + c) = 1u;
+                        }
+                    }
                 }
             }
             if (state != kActive && state != kHeld) state = kIdle;
@@ -262,6 +311,20 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
                 if (lane == leader) got = atomicAdd(ticket, (unsigned long long)__popc(idle));
                 got = __shfl_sync(kFull, got, leader);
                 if (got + __popc(idle) >= (unsigned long long)count) more = false;
+                if (STREAM && got < (unsigned long long)count) {
+                    // streamed batch: the records handed out must have arrived
+                    const int64_t last = (int64_t)min(got + (unsigned long long)__popc(idle),
+                                                      (unsigned long long)count) - 1;
+                    const int64_t c_last = last / ls.chunk;
+                    if (c_last > ready_upto) {
+                        bool ok = true;
+                        if (lane == 0) ok = wait_chunk(ls.chunk_ready, c_last);
+                        ok = __shfl_sync(kFull, ok, 0);
+                        if (!ok && lane == 0) atomicOr(b.error, kErrWait);
+                        ready_upto = c_last;
+                        __syncwarp();
+                    }
+                }
                 if (state == kIdle) {
                     const unsigned long long pos = got + __popc(idle & ((1u << lane) - 1u));
                     if (pos < (unsigned long long)count) {
@@ -317,9 +380,11 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
                         for (int v = 0; v < 16; ++v) tb[(c * 16 + v) * 32] = t[v];
                     }
                     if (bad) {
-                        if (b.out_len) b.out_len[k] = kLenInvalid;
+                        // written (and counted) at the next refill pass
                         atomicOr(b.error, kErrInvalid);
-                        state = kIdle;
+                        state = kDone;
+                        res_len = kLenInvalid;
+                        res_word = 0;
                     } else {
 #pragma unroll 16
                         for (int w = 0; w < BW; ++w) bm[w * 32] = 0u;
@@ -338,17 +403,20 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
                 // first of the automata this warp kept
                 for (unsigned held = __ballot_sync(kFull, state == kHeld); held; held &= held - 1u) {
                     const int64_t e = __shfl_sync(kFull, k, __ffs(held) - 1);
-                    warp_solve<NMAX, WORDS>(b, e, base, lane, expanded);
+                    const unsigned long long slot = __shfl_sync(kFull, hslot, __ffs(held) - 1);
+                    warp_solve<NMAX, WORDS, STREAM>(b, e, base, lane, expanded, ls, slot);
                 }
                 if (state == kHeld) state = kIdle;
                 if (!more) {
                     // no new automata either: solve escalated ones while any can be claimed
                     while (true) {
                         int64_t e = -1;
-                        if (lane == 0) e = claim_escalated(escal_list, escal_capacity, escal_claim);
+                        unsigned long long slot = 0;
+                        if (lane == 0) e = claim_escalated(escal_list, escal_capacity, escal_claim, slot);
                         e = __shfl_sync(kFull, e, 0);
+                        slot = __shfl_sync(kFull, slot, 0);
                         if (e < 0) break;
-                        warp_solve<NMAX, WORDS>(b, e, base, lane, expanded);
+                        warp_solve<NMAX, WORDS, STREAM>(b, e, base, lane, expanded, ls, slot);
                     }
                     break;
                 }
@@ -429,16 +497,19 @@ size_t smem_for(int warps, int ring)
 template <int NMAX, bool WORDS>
 cudaError_t launch_t(int warps, int ring, int refill_k, int tail_k, int ctas, const Batch &b, int32_t *escal_list,
                      unsigned long long escal_capacity, unsigned long long *escal_count,
-                     unsigned long long *escal_claim, unsigned long long *ticket, cudaStream_t st)
+                     unsigned long long *escal_claim, unsigned long long *ticket, const LaneStream &ls,
+                     cudaStream_t st)
 {
     using G = LaneGeom<NMAX>;
     // the warp-cooperative search needs the bitmap and 2^NMAX queue entries in one region
     static_assert(G::kTable * 32 >= G::kBitmapWords, "region too small for the warp search");
     const size_t smem = smem_for<NMAX>(warps, ring);
-    cudaError_t e = cudaFuncSetAttribute(k_lane<NMAX, WORDS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // the streamed form's bookkeeping is compiled out of the resident-batch kernel
+    auto kernel = ls.chunk_done ? k_lane<NMAX, WORDS, true> : k_lane<NMAX, WORDS, false>;
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_lane<NMAX, WORDS><<<ctas, warps * 32, smem, st>>>(b, ring, refill_k, tail_k, escal_list, escal_capacity,
-                                                       escal_count, escal_claim, ticket);
+    kernel<<<ctas, warps * 32, smem, st>>>(b, ring, refill_k, tail_k, escal_list, escal_capacity, escal_count,
+                                           escal_claim, ticket, ls);
     return cudaGetLastError();
 }
 
@@ -451,7 +522,7 @@ size_t lane_smem_bytes(int nmax, int warps, int ring)
 
 int lane_max_ctas_per_sm(int nmax, int warps, int ring)
 {
-    const void *k = nmax <= 8 ? (const void *)k_lane<8, true> : (const void *)k_lane<12, true>;
+    const void *k = nmax <= 8 ? (const void *)k_lane<8, true, false> : (const void *)k_lane<12, true, false>;
     const size_t smem = lane_smem_bytes(nmax, warps, ring);
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         cudaGetLastError();
@@ -465,24 +536,52 @@ int lane_max_ctas_per_sm(int nmax, int warps, int ring)
     return blocks;
 }
 
+// Streamed batches: after the chunk copies, the escalated automata's results
+// (solved late, after their chunk may already have been copied) are stored
+// straight into the host's mapped output.
+__global__ void k_escal_patch(const EscalResult *r, const unsigned long long *count, int32_t *len, uint64_t *words,
+                              int ws)
+{
+    const int64_t n = (int64_t)*count;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const EscalResult e = r[i];
+        if (len) len[e.k] = e.len;
+        if (words) {
+            uint64_t *w = words + (size_t)e.k * (size_t)ws;
+            w[0] = e.word[0];
+            if (ws > 1) w[1] = e.word[1];
+            for (int j = 2; j < ws; ++j) w[j] = 0ull;
+        }
+    }
+}
+
+cudaError_t launch_escal_patch(const EscalResult *r, const unsigned long long *count, int32_t *len, uint64_t *words,
+                               int ws, int sm_count, cudaStream_t st)
+{
+    k_escal_patch<<<2 * sm_count, 256, 0, st>>>(r, count, len, words, ws);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_lane(int nmax, int warps, int ring, int refill_k, int tail_k, int ctas, const Batch &b,
                         int32_t *escal_list, unsigned long long escal_capacity, unsigned long long *escal_count,
-                        unsigned long long *escal_claim, unsigned long long *ticket, cudaStream_t st)
+                        unsigned long long *escal_claim, unsigned long long *ticket, const LaneStream &ls,
+                        cudaStream_t st)
 {
     if ((ring & (ring - 1)) || ring < 8 || warps < 1 || warps > 8 || ctas < 1 || refill_k < 1 || refill_k > 32 ||
         tail_k < 0 || tail_k > 32)
         return cudaErrorInvalidValue;
+    if (ls.chunk_done && (ls.chunk < 1 || b.order || b.range_dev)) return cudaErrorInvalidValue;
     const bool words = b.out_words != nullptr;
     if (nmax <= 8)
         return words ? launch_t<8, true>(warps, ring, refill_k, tail_k, ctas, b, escal_list, escal_capacity,
-                                         escal_count, escal_claim, ticket, st)
+                                         escal_count, escal_claim, ticket, ls, st)
                      : launch_t<8, false>(warps, ring, refill_k, tail_k, ctas, b, escal_list, escal_capacity,
-                                          escal_count, escal_claim, ticket, st);
+                                          escal_count, escal_claim, ticket, ls, st);
     if (nmax <= 12)
         return words ? launch_t<12, true>(warps, ring, refill_k, tail_k, ctas, b, escal_list, escal_capacity,
-                                          escal_count, escal_claim, ticket, st)
+                                          escal_count, escal_claim, ticket, ls, st)
                      : launch_t<12, false>(warps, ring, refill_k, tail_k, ctas, b, escal_list, escal_capacity,
-                                           escal_count, escal_claim, ticket, st);
+                                           escal_count, escal_claim, ticket, ls, st);
     return cudaErrorInvalidValue;
 }
 

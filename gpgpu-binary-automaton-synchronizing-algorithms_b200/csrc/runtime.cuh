@@ -50,6 +50,18 @@ struct HostBuf {
     template <class T> T *as() const { return static_cast<T *>(ptr); }
 };
 
+// The streamed host path (uniform n <= 12 on the per-lane kernel): records go
+// in chunk by chunk on the handle's copy-in stream while one kernel runs, and
+// each chunk's results come back on copy_out as soon as the kernel flags it.
+struct Streamer {
+    cudaStream_t copy_out = nullptr;
+    cudaEvent_t ev_in0 = nullptr, ev_kdone = nullptr;
+    DevBuf flags;        // chunk_ready[nch] | chunk_done[nch]
+    DevBuf escal_out;    // EscalResult per escalation slot
+    HostBuf h_flags;     // host_flag[nch] | zeros[nch] | ones[nch] (mapped)
+    HostBuf h_escal;     // escal_out copied back
+};
+
 // Parameters of the one-automaton-per-lane kernel (classes 0 and 1).
 struct LaneShape {
     int nmax;       // 8 or 12
@@ -143,6 +155,7 @@ struct sbfs_handle {
     // chunk order, so the first chunk's kernels start after one chunk's copy
     // rather than after all lanes' copies have shared the link
     cudaStream_t copy_in = nullptr;
+    sbfs::Streamer streamer;
     sbfs::Plan plan{};
     bool plan_ready = false;
     // last sbfs_solve_batch_device call: lane 0's buffers are in use until ev_device

@@ -272,3 +272,56 @@ def test_level_slots_recycle_under_load(oracle_mod):
     ref = oracle_mod.solve(recs, n=21, words=False, threads=16)
     np.testing.assert_array_equal(r["len"], ref["len"])
     assert oracle_mod.replay(recs, r["len"], r["words"], n=21)[0] == 0
+
+
+@pytest.mark.parametrize("n,count", [(12, 300_001), (8, 262_145), (11, 1_000_003)])
+def test_streamed_host_path(oracle_mod, n, count):
+    """Uniform n <= 12 batches of at least two 2^17-automaton chunks take the
+    streamed host path (one kernel, chunked copies both ways, escalated
+    automata patched in at the end); an explicit chunk size takes the
+    chunked multi-stream path.  Both must match the oracle."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from sbfs import dotnet_random as D
+    recs = D.fill_array_of_problems(count, n, 777 + n, lstride=n)
+    ref = oracle_mod.solve(recs, n=n, lstride=n, words=False, threads=8)
+    with sbfs.Engine(device=0) as eng, sbfs.Engine(device=0, chunk=1 << 16) as chunked:
+        r = eng.solve(recs, n=n, lstride=n)
+        _check(oracle_mod, recs, r, n=n, lstride=n, ref=ref)
+        # the streamed path: one BFS kernel, the result count, the escalated-result patch
+        assert r["stats"]["launches"] <= 3
+        # pinned host buffers (direct copies) give the same lengths; words replay
+        pin = torch.from_numpy(recs).pin_memory()
+        out_len = torch.empty(count, dtype=torch.int32).pin_memory()
+        out_words = torch.empty((count, r["word_stride"]), dtype=torch.int64).pin_memory()
+        p = eng.solve(pin.numpy(), n=n, lstride=n, out=(out_len.numpy(), out_words.numpy().view(np.uint64)))
+        np.testing.assert_array_equal(p["len"], ref["len"])
+        assert oracle_mod.replay(recs, p["len"], p["words"], n=n, lstride=n)[0] == 0
+        v = eng.verify(recs, n=n, lstride=n)
+        np.testing.assert_array_equal(v["len"], ref["len"])
+        assert eng.verify(recs, n=n, lstride=n, lengths=False)["first_violation"] == -1
+        c = chunked.solve(recs, n=n, lstride=n)
+        np.testing.assert_array_equal(c["len"], ref["len"])
+        assert c["stats"]["launches"] > 3
+
+
+def test_streamed_path_violation_and_malformed(oracle_mod):
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from sbfs import dotnet_random as D
+    count = 400_000
+    recs = D.fill_array_of_problems(count, 12, 4242, lstride=12)
+    recs[333_333] = P.repack(P.cerny_record(12)[None, :], 32, 12)[0]
+    with sbfs.Engine(device=0, slack=1) as eng:
+        v = eng.verify(recs, n=12, lstride=12)
+        assert v["first_violation"] == 333_333 and v["len"][333_333] == 121
+    bad = recs.copy()
+    bad[299_999, 3] = 12   # state 12 in a 12-state automaton
+    with sbfs.Engine(device=0) as eng:
+        with pytest.raises(sbfs.SbfsError) as ei:
+            eng.solve(bad, n=12, lstride=12)
+        assert ei.value.status == 1
+        r = eng.solve(recs, n=12, lstride=12)   # the handle stays usable
+        assert r["first_violation"] == -1 and r["len"][333_333] == 121
