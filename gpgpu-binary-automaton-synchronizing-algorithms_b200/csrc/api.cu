@@ -334,8 +334,8 @@ sbfs_status ensure_plan(sbfs_handle *h)
     }
     const int lane_defaults[2][4] = {
         // warps, ring, refill_k, tail_k (the autotuner's picks on B200 for uniform n = 8 and n = 12)
-        {8, 16, 16, 8},
-        {1, 64, 16, 8},
+        {8, 16, 16, 4},
+        {1, 64, 16, 4},
     };
     for (int c = 0; c < 2; ++c) {
         LaneShape &ls = P.lane[c];

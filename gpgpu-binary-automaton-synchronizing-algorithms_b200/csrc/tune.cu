@@ -80,7 +80,7 @@ std::string device_key(sbfs_handle *h)
     cudaDeviceProp p;
     cudaGetDeviceProperties(&p, h->device);
     char buf[320];
-    std::snprintf(buf, sizeof buf, "%s|sm%d|abi%d|v6", p.name, h->sm_count, SBFS_ABI_VERSION);
+    std::snprintf(buf, sizeof buf, "%s|sm%d|abi%d|v7", p.name, h->sm_count, SBFS_ABI_VERSION);
     for (char *c = buf; *c; ++c)
         if (*c == ' ') *c = '_';
     return buf;
@@ -193,7 +193,7 @@ cudaError_t plan_autotune(sbfs_handle *h, Plan &plan)
         for (int w : warps_c[c])
             for (int ring : {16, 32, 64})
                 for (int rk : {8, 16})
-                    for (int tk : {0, 8, 16}) {
+                    for (int tk : {0, 4, 8}) {
                         if (!w) continue;
                         Plan t = P;
                         t.use_pool[c] = 0;
