@@ -61,6 +61,8 @@ def parse_args():
     ap.add_argument("--rates", default="2000,8000,32000,128000,0",
                     help="serving: offered request rates per second (0 = submit all at once)")
     ap.add_argument("--count", type=int, default=0, help="automata per GPU (0 = the workload's size)")
+    ap.add_argument("--max-batch", type=int, default=0, help="serving: small requests per mini-batch (0 = 8192)")
+    ap.add_argument("--max-levels", type=int, default=0, help="serving: levels per launch batch (0 = 16)")
     ap.add_argument("--inputs", choices=["reference", "hash"], default="reference",
                     help="n12/n8: the reference's System.Random batch or a counter-hash batch")
     ap.add_argument("--cpu-seconds", type=float, default=1.5, help="wall time of the CPU baseline sample")
@@ -480,7 +482,7 @@ def run_serving(args):
     rates = [float(r) for r in args.rates.split(",")]
     rng = np.random.default_rng(seed)
     sweep = []
-    srv = Server(device=0)
+    srv = Server(device=0, max_batch=args.max_batch, max_levels=args.max_levels)
     # warm-up: every path once
     warm = [srv.submit(a_rows[i], b_rows[i], int(ns[i])) for i in range(0, min(count, 2000), 7)]
     srv.wait_all(warm)
@@ -524,6 +526,8 @@ def run_serving(args):
         by_id = [results[i] for i in ids]
         lat = np.array([r["done_ms"] - r["submit_ms"] for r in by_id])
         small = np.array([int(r["n"]) <= 20 for r in by_id])
+        tiny = np.array([int(r["n"]) <= 16 for r in by_id])
+        mid = small & ~tiny
         first = min(r["submit_ms"] for r in by_id)
         last = max(r["done_ms"] for r in by_id)
         entry = {
@@ -533,6 +537,10 @@ def run_serving(args):
                            "max": float(lat.max())},
             "latency_ms_n_le_20": {"p50": float(np.percentile(lat[small], 50)),
                                    "p99": float(np.percentile(lat[small], 99))},
+            "latency_ms_n_le_16": {"p50": float(np.percentile(lat[tiny], 50)),
+                                   "p99": float(np.percentile(lat[tiny], 99))},
+            "latency_ms_n_17_20": {"p50": float(np.percentile(lat[mid], 50)),
+                                   "p99": float(np.percentile(lat[mid], 99))},
             "peak_arena_bytes": int(st["arena_peak"]), "submit_retries": refused[0], "wall_s": wall,
         }
         sweep.append(entry)

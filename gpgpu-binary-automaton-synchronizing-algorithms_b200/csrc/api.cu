@@ -135,6 +135,8 @@ struct Job {
     int32_t *len;            // device or null
     uint64_t *words;         // device or null
     int32_t word_stride;
+    unsigned int *done_flag = nullptr;   // per-automaton completion flags (serving)
+    unsigned int done_tag = 0;
 };
 
 int class_present_mask(const Job &j)
@@ -246,6 +248,8 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
     b.first_violation = &ctr->first_violation;
     b.expanded = &ctr->expanded;
     b.error = &ctr->error;
+    b.done_flag = j.done_flag;
+    b.done_tag = j.done_tag;
 
     const int present = class_present_mask(j);
     const size_t escal_entries = (size_t)std::max<int64_t>(j.count, 1);
@@ -296,7 +300,7 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
         }
         *launches += 1;
     }
-    if (!plain && j.len && j.count > 0) {
+    if (!plain && j.len && j.count > 0 && !j.done_flag) {
         CK(launch_count_sync(j.len, j.count, &ctr->synchronizing, h->sm_count, st), "launching result count");
         *launches += 1;
     }
@@ -929,12 +933,13 @@ namespace sbfs {
 // reset, size-class bucketing, class kernels).  Shared with the serving loop.
 sbfs_status engine_enqueue(sbfs_handle *h, Lane &L, const uint8_t *d_maps, int32_t lstride, const uint8_t *d_ns,
                            int32_t n_uniform, int32_t max_n, int64_t count, int32_t *d_len, uint64_t *d_words,
-                           int32_t word_stride, int *launches)
+                           int32_t word_stride, int *launches, unsigned int *done_flag, unsigned int done_tag)
 {
     sbfs_status s = ensure_plan(h);
     if (s) return s;
     if ((s = reset_counters(h, L))) return s;
-    Job j{d_maps, lstride, d_ns, n_uniform, max_n, count, d_len, d_words, d_words ? word_stride : 0};
+    Job j{d_maps, lstride, d_ns, n_uniform, max_n, count, d_len, d_words, d_words ? word_stride : 0, done_flag,
+          done_tag};
     return enqueue_kernels(h, L, j, launches);
 }
 

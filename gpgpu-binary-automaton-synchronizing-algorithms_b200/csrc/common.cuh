@@ -37,6 +37,12 @@ struct Batch {
     unsigned long long *first_violation;   // atomicMin target, starts at ULLONG_MAX
     unsigned long long *expanded;          // stats counter (nullable)
     int *error;                            // error bits
+    // Per-automaton completion (serving): after an automaton's length and
+    // word are stored, done_flag[k] = done_tag (nonzero, new per launch).
+    // out_len / out_words may then be mapped host memory the host reads as
+    // soon as the flag appears.  nullptr = no flags.
+    unsigned int *done_flag;
+    unsigned int done_tag;
 };
 
 __device__ __forceinline__ int automaton_n(const Batch &b, int64_t k)
@@ -69,6 +75,15 @@ __device__ __forceinline__ int cerny_bound(int n, int slack)
 __device__ __forceinline__ bool is_singleton(uint32_t s)
 {
     return (s & (s - 1u)) == 0u;
+}
+
+// Called once the automaton's length and word are stored.
+__device__ __forceinline__ void publish_result(const Batch &b, int64_t k)
+{
+    if (b.done_flag) {
+        __threadfence_system();
+        *(volatile unsigned int *)(b.done_flag + k) = b.done_tag;
+    }
 }
 
 __device__ __forceinline__ void record_result(const Batch &b, int64_t k, int n, int32_t len)

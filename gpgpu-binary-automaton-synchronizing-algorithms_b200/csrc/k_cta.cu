@@ -68,6 +68,7 @@ __global__ void __launch_bounds__(1024) k_cta(Batch b, int nb_max, uint64_t *que
             if (tid == 0) {
                 if (b.out_len) b.out_len[k] = kLenInvalid;
                 atomicOr(b.error, kErrInvalid);
+                publish_result(b, k);
             }
             __syncthreads();
             continue;
@@ -166,6 +167,7 @@ __global__ void __launch_bounds__(1024) k_cta(Batch b, int nb_max, uint64_t *que
                             }
                         }
                     }
+                    publish_result(b, k);
                 }
                 break;
             }
@@ -176,6 +178,7 @@ __global__ void __launch_bounds__(1024) k_cta(Batch b, int nb_max, uint64_t *que
                         uint64_t *w = b.out_words + (size_t)k * (size_t)b.word_stride;
                         for (int c = 0; c < b.word_stride; ++c) w[c] = 0ull;
                     }
+                    publish_result(b, k);
                 }
                 break;
             }

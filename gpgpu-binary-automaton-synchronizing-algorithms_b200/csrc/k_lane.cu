@@ -212,6 +212,7 @@ __device__ void warp_solve(const Batch &b, int64_t k, uint32_t *region, int lane
             r.word[1] = w1;
             ls.escal_out[slot] = r;
         }
+        publish_result(b, k);
     }
     __syncwarp();
 }
@@ -269,6 +270,7 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
                     w[0] = res_len > 0 ? (uint64_t)res_word : 0ull;
                     for (int c = 1; c < b.word_stride; ++c) w[c] = 0ull;
                 }
+                publish_result(b, k);
             }
             const unsigned esc = __ballot_sync(kFull, state == kEscalate);
             if (esc) {

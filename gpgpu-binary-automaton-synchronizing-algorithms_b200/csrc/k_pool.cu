@@ -133,6 +133,7 @@ __global__ void __launch_bounds__(512) k_pool(Batch b, int q_smem, int grab, uin
                 if (lane == 0) {
                     if (b.out_len) b.out_len[k] = kLenInvalid;
                     atomicOr(b.error, kErrInvalid);
+                    publish_result(b, k);
                 }
                 continue;   // slot s stays free
             }
@@ -292,6 +293,7 @@ __global__ void __launch_bounds__(512) k_pool(Batch b, int q_smem, int grab, uin
                 }
                 for (int c = top + 1; c < ws; ++c) w[c] = 0ull;
             }
+            publish_result(b, my_k);
         }
         unsigned done_mask = __ballot_sync(kFull, done);
         while (done_mask) {

@@ -89,7 +89,9 @@ private:
 // Host engine of one set of level slots on one stream.
 class LevelEngine {
 public:
-    cudaError_t init(int sm_count, size_t arena_bytes, cudaStream_t st);
+    // with `shared`, slots are carved from that arena (reserved by its owner,
+    // possibly shared with other engines) and arena_bytes is ignored
+    cudaError_t init(int sm_count, size_t arena_bytes, cudaStream_t st, Arena *shared = nullptr);
     void destroy();
     // bytes an automaton with n states needs (bitmap + full-size queue), 256-aligned
     static size_t footprint(int n);
@@ -121,11 +123,11 @@ public:
         return true;
     }
     bool launched() const { return launched_; }
-    void reset_peak() { arena_.reset_peak(); }
+    void reset_peak() { arena().reset_peak(); }
     int in_flight() const { return in_flight_; }
-    size_t arena_used() const { return arena_.used(); }
-    size_t arena_peak() const { return arena_.peak(); }
-    size_t arena_capacity() const { return arena_.capacity(); }
+    size_t arena_used() const { return arena().used(); }
+    size_t arena_peak() const { return arena().peak(); }
+    size_t arena_capacity() const { return arena().capacity(); }
     unsigned long long expanded() const { return expanded_; }
     int launches() const { return launches_; }
     cudaStream_t stream() const { return st_; }
@@ -140,7 +142,10 @@ private:
     LevelSlot *h_slots_ = nullptr;   // pinned mirror
     LevelCtl *h_ctl_ = nullptr;      // pinned mirror
     int *h_init_ = nullptr;          // pinned: nslots, n_init, init_list[]
-    Arena arena_;
+    Arena own_;
+    Arena *shared_ = nullptr;
+    Arena &arena() { return shared_ ? *shared_ : own_; }
+    const Arena &arena() const { return shared_ ? *shared_ : own_; }
     std::vector<size_t> slot_off_;   // arena offset per slot (SIZE_MAX = free)
     std::vector<int> pending_init_;
     int nslots_ = 0;

@@ -82,9 +82,10 @@ size_t LevelEngine::footprint(int n)
     return ((bitmap + 255) & ~size_t(255)) + ((queue + 255) & ~size_t(255));
 }
 
-cudaError_t LevelEngine::init(int sm_count, size_t arena_bytes, cudaStream_t st)
+cudaError_t LevelEngine::init(int sm_count, size_t arena_bytes, cudaStream_t st, Arena *shared)
 {
     st_ = st;
+    shared_ = shared;
     cudaError_t e;
     const int per_sm = level_max_ctas_per_sm();
     ctas_ = (per_sm > 0 ? per_sm : 1) * sm_count;
@@ -107,7 +108,7 @@ cudaError_t LevelEngine::init(int sm_count, size_t arena_bytes, cudaStream_t st)
     nslots_ = 0;
     in_flight_ = 0;
     parity_ = 0;
-    return arena_.reserve(arena_bytes);
+    return shared_ ? cudaSuccess : own_.reserve(arena_bytes);
 }
 
 void LevelEngine::destroy()
@@ -120,7 +121,7 @@ void LevelEngine::destroy()
     if (h_ctl_) cudaFreeHost(h_ctl_);
     if (h_init_) cudaFreeHost(h_init_);
     if (ev_) cudaEventDestroy(ev_);
-    arena_.release();
+    own_.release();
     d_slots_ = nullptr;
     d_tables_ = nullptr;
     d_ctl_ = nullptr;
@@ -141,15 +142,15 @@ int LevelEngine::admit(const uint8_t *d_rec, int lstride, int n, long long tag, 
         }
     if (s < 0) return -1;
     const size_t fp = footprint(n);
-    const size_t off = arena_.alloc(fp);
+    const size_t off = arena().alloc(fp);
     if (off == SIZE_MAX) return -1;
     slot_off_[s] = off;
     LevelSlot &sl = h_slots_[s];
     std::memset(&sl, 0, sizeof(sl));
     const size_t bitmap = ((n >= 7 ? ((size_t)1 << n) / 8 : 16) + 255) & ~size_t(255);
     sl.rec = d_rec;
-    sl.bitmap = reinterpret_cast<uint32_t *>(arena_.base() + off);
-    sl.queue = reinterpret_cast<uint64_t *>(arena_.base() + off + bitmap);
+    sl.bitmap = reinterpret_cast<uint32_t *>(arena().base() + off);
+    sl.queue = reinterpret_cast<uint64_t *>(arena().base() + off + bitmap);
     sl.cap = (unsigned long long)1 << n;
     sl.tag = tag;
     sl.n = n;
@@ -234,7 +235,7 @@ cudaError_t LevelEngine::collect(std::vector<Finished> &done)
             f.state = sl.state;
             std::memcpy(f.word, sl.word, sizeof(f.word));
             done.push_back(f);
-            arena_.free(slot_off_[s]);
+            arena().free(slot_off_[s]);
             slot_off_[s] = SIZE_MAX;
             sl.state = kSlotFree;   // the device copy stays Done, which the kernel ignores
             --in_flight_;

@@ -138,9 +138,13 @@ struct Plan {
 struct sbfs_handle;
 
 namespace sbfs {
+// With done_flag, d_len / d_words may be mapped host memory: every automaton's
+// result is stored there and then flagged (done_flag[i] = done_tag) as soon as
+// it is known, before the launch sequence as a whole completes.
 sbfs_status engine_enqueue(sbfs_handle *h, Lane &L, const uint8_t *d_maps, int32_t lstride, const uint8_t *d_ns,
                            int32_t n_uniform, int32_t max_n, int64_t count, int32_t *d_len, uint64_t *d_words,
-                           int32_t word_stride, int *launches);
+                           int32_t word_stride, int *launches, unsigned int *done_flag = nullptr,
+                           unsigned int done_tag = 0);
 }  // namespace sbfs
 
 struct sbfs_handle {

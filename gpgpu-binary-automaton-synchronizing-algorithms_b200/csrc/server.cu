@@ -4,16 +4,24 @@
 // One loop thread owns the GPU work; submit/poll/cancel only touch queues
 // under a mutex.  Each turn of the loop:
 //   * takes newly submitted requests;
-//   * small requests (n <= 16): when the previous mini-batch is done, packs up
-//     to max_batch of them into pinned 64-byte records, copies them in, runs
-//     the batch kernels (per-lane / warp-pooled) on its own stream and copies
-//     lengths and words back; a mini-batch completes in one launch sequence;
+//   * small requests (n <= 16): whenever one of kSmallSlots mini-batch slots is
+//     free, packs up to max_batch of them into pinned 64-byte records, copies
+//     them in and runs the batch kernels (per-lane / warp-pooled) on the
+//     slot's own stream.  The kernels store each automaton's length and word
+//     straight into mapped host memory and then flag it, so every request is
+//     delivered as soon as its own search ends -- a mini-batch holding a
+//     2^16-subset Cerny search does not hold back the other requests in it;
 //   * large requests (n >= 17): when the previous level launch batch is done,
 //     collects finished slots, admits waiting requests in arrival order while
 //     their bitmap + queue fit the arena (the 2^n-bit budget), and launches
 //     the next few levels of every admitted request (k_level.cu).  Requests
 //     that arrive while others are running are admitted at the next turn and
 //     advance together with them: their work overlaps on the device.
+//     n = 17..20 and n >= 21 run on two level engines with their own streams
+//     (the first at higher priority) and one shared arena, so an n <= 20
+//     request never waits for the wide levels of a 2^24-subset search; the
+//     big engine leaves a reserve of the arena to the first while it has
+//     anything admitted.
 // Completion order follows the GPU, not submission order.
 #include <atomic>
 #include <chrono>
@@ -40,7 +48,26 @@ struct Request {
 };
 
 constexpr int kSmallMaxN = 16;
+constexpr int kMidMaxN = 20;
 constexpr int kWords = 12;
+constexpr int kSmallSlots = 4;   // mini-batches in flight (lanes 0..3; then n <= 20 and n >= 21 slots)
+
+// One mini-batch of small requests in flight.
+struct SmallSlot {
+    int lane = 0;                        // handle lane: stream and kernel scratch
+    DevBuf d_recs, d_ns;
+    HostBuf h_recs, h_ns;                // staging in
+    HostBuf h_len, h_words, h_flags;     // mapped: the kernels store results and flags here
+    int32_t *dl = nullptr;               // device aliases of the mapped buffers
+    uint64_t *dw = nullptr;
+    unsigned int *df = nullptr;
+    std::vector<Request> reqs;
+    std::vector<char> delivered;
+    size_t left = 0;                     // requests not yet delivered
+    unsigned int tag = 0;                // this launch's flag value
+    cudaEvent_t ev = nullptr;
+    bool busy = false;
+};
 
 }  // namespace
 
@@ -60,13 +87,11 @@ struct sbfs_server {
     // stats (mutex-protected)
     sbfs_server_stats st{};
     // loop-owned
-    std::deque<Request> pend_small, pend_large;
-    std::vector<Request> small_batch;
-    bool small_busy = false;
-    cudaEvent_t small_ev = nullptr;
-    DevBuf d_recs, d_ns, d_len, d_words;
-    HostBuf h_recs, h_ns, h_len, h_words;
-    LevelEngine level;
+    std::deque<Request> pend_small, pend_mid, pend_big;
+    SmallSlot small[kSmallSlots];
+    unsigned int next_tag = 1;
+    Arena arena;                                   // shared by both level engines
+    LevelEngine mid, big;                          // n = 17..20 / n >= 21
     std::unordered_map<long long, Request> large;   // admitted, keyed by id
     std::string error;
 
@@ -96,58 +121,76 @@ void complete(sbfs_server *s, const Request &r, int32_t status, int32_t len, con
     s->cv_out.notify_all();
 }
 
-bool launch_small(sbfs_server *s)
+bool event_done(cudaEvent_t ev);
+
+bool launch_small(sbfs_server *s, SmallSlot &S)
 {
-    Lane &L = s->h->lanes[0];
+    Lane &L = s->h->lanes[(size_t)S.lane];
     const int cap = s->cfg.max_batch;
-    s->small_batch.clear();
-    while (!s->pend_small.empty() && (int)s->small_batch.size() < cap) {
-        s->small_batch.push_back(s->pend_small.front());
+    S.reqs.clear();
+    while (!s->pend_small.empty() && (int)S.reqs.size() < cap) {
+        S.reqs.push_back(s->pend_small.front());
         s->pend_small.pop_front();
     }
-    const int64_t cnt = (int64_t)s->small_batch.size();
+    const int64_t cnt = (int64_t)S.reqs.size();
     if (!cnt) return false;
-    uint8_t *rec = s->h_recs.as<uint8_t>();
-    uint8_t *ns = s->h_ns.as<uint8_t>();
+    uint8_t *rec = S.h_recs.as<uint8_t>();
+    uint8_t *ns = S.h_ns.as<uint8_t>();
     int max_n = 1;
     for (int64_t i = 0; i < cnt; ++i) {
-        const Request &r = s->small_batch[(size_t)i];
+        const Request &r = S.reqs[(size_t)i];
         std::memset(rec + i * 64, 0, 64);
         std::memcpy(rec + i * 64, r.a, (size_t)r.n);
         std::memcpy(rec + i * 64 + 32, r.b, (size_t)r.n);
         ns[i] = (uint8_t)r.n;
         max_n = std::max(max_n, r.n);
     }
+    S.tag = s->next_tag++;
+    if (s->next_tag == 0) s->next_tag = 1;
     cudaStream_t st = L.stream;
-    cudaMemcpyAsync(s->d_recs.ptr, rec, (size_t)cnt * 64, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(s->d_ns.ptr, ns, (size_t)cnt, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(S.d_recs.ptr, rec, (size_t)cnt * 64, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(S.d_ns.ptr, ns, (size_t)cnt, cudaMemcpyHostToDevice, st);
     int launches = 0;
-    sbfs_status e = engine_enqueue(s->h, L, s->d_recs.as<uint8_t>(), 32, s->d_ns.as<uint8_t>(), 0, max_n, cnt,
-                                   s->d_len.as<int32_t>(), s->d_words.as<uint64_t>(), kWords, &launches);
+    sbfs_status e = engine_enqueue(s->h, L, S.d_recs.as<uint8_t>(), 32, S.d_ns.as<uint8_t>(), 0, max_n, cnt, S.dl,
+                                   S.dw, kWords, &launches, S.df, S.tag);
     if (e != SBFS_OK) {
         s->error = s->h->last_error;
-        for (const Request &r : s->small_batch) complete(s, r, e, -1, nullptr);
-        s->small_batch.clear();
+        for (const Request &r : S.reqs) complete(s, r, e, -1, nullptr);
+        S.reqs.clear();
         return false;
     }
-    cudaMemcpyAsync(s->h_len.ptr, s->d_len.ptr, (size_t)cnt * sizeof(int32_t), cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(s->h_words.ptr, s->d_words.ptr, (size_t)cnt * kWords * sizeof(uint64_t), cudaMemcpyDeviceToHost,
-                    st);
-    cudaEventRecord(s->small_ev, st);
-    s->small_busy = true;
+    cudaEventRecord(S.ev, st);
+    S.delivered.assign((size_t)cnt, 0);
+    S.left = (size_t)cnt;
+    S.busy = true;
     std::lock_guard<std::mutex> lock(s->mu);
     s->st.small_batches++;
     return true;
 }
 
-void finish_small(sbfs_server *s)
+// Delivers the slot's requests whose flags are up; frees the slot once its
+// launch sequence has completed.
+bool poll_small(sbfs_server *s, SmallSlot &S)
 {
-    const int32_t *len = s->h_len.as<int32_t>();
-    const uint64_t *words = s->h_words.as<uint64_t>();
-    for (size_t i = 0; i < s->small_batch.size(); ++i)
-        complete(s, s->small_batch[i], SBFS_OK, len[i], words + i * kWords);
-    s->small_batch.clear();
-    s->small_busy = false;
+    bool progress = false;
+    const volatile unsigned int *flag = S.h_flags.as<unsigned int>();
+    const int32_t *len = S.h_len.as<int32_t>();
+    const uint64_t *words = S.h_words.as<uint64_t>();
+    const bool finished = event_done(S.ev);   // sampled before the flags: all are up once it is done
+    for (size_t i = 0; i < S.reqs.size() && S.left; ++i) {
+        if (S.delivered[i] || (flag[i] != S.tag && !finished)) continue;
+        std::atomic_thread_fence(std::memory_order_acquire);
+        complete(s, S.reqs[i], SBFS_OK, len[i], words + i * kWords);
+        S.delivered[i] = 1;
+        --S.left;
+        progress = true;
+    }
+    if (finished) {
+        S.reqs.clear();
+        S.busy = false;
+        progress = true;
+    }
+    return progress;
 }
 
 bool event_done(cudaEvent_t ev)
@@ -169,8 +212,10 @@ void run_loop(sbfs_server *s)
         bool progress = false;
         {
             std::unique_lock<std::mutex> lock(s->mu);
-            if (s->incoming.empty() && s->pend_small.empty() && s->pend_large.empty() && !s->small_busy &&
-                s->large.empty()) {
+            bool small_busy = false;
+            for (const SmallSlot &S : s->small) small_busy |= S.busy;
+            if (s->incoming.empty() && s->pend_small.empty() && s->pend_mid.empty() && s->pend_big.empty() &&
+                !small_busy && s->large.empty()) {
                 if (s->stopping) break;
                 s->cv_in.wait_for(lock, std::chrono::milliseconds(2));
             }
@@ -183,53 +228,64 @@ void run_loop(sbfs_server *s)
                     lock.lock();
                     continue;
                 }
-                (r.n <= kSmallMaxN ? s->pend_small : s->pend_large).push_back(r);
+                (r.n <= kSmallMaxN ? s->pend_small : r.n <= kMidMaxN ? s->pend_mid : s->pend_big).push_back(r);
                 progress = true;
             }
         }
         // small path
-        if (s->small_busy && event_done(s->small_ev)) {
-            finish_small(s);
-            progress = true;
-        }
-        if (!s->small_busy && !s->pend_small.empty()) progress |= launch_small(s);
-        // large path
-        if (s->level.launched() && s->level.ready()) {
-            fin.clear();
-            s->level.collect(fin);
-            for (auto &f : fin) {
-                auto it = s->large.find(f.tag);
-                if (it == s->large.end()) continue;
-                complete(s, it->second, f.state == kSlotDone ? SBFS_OK : SBFS_ECUDA, f.len, f.word);
-                s->large.erase(it);
-            }
-            progress = true;
-        }
-        if (!s->level.launched()) {
-            while (!s->pend_large.empty()) {
-                const Request &r = s->pend_large.front();
-                if (s->level.admit(nullptr, 32, r.n, (long long)r.id, r.a, r.b) < 0) break;
-                s->large.emplace((long long)r.id, r);
-                s->pend_large.pop_front();
-            }
-            if (s->level.in_flight() > 0) {
-                s->level.launch(s->cfg.max_levels, none, 4 * s->cfg.max_levels);
-                std::lock_guard<std::mutex> lock(s->mu);
-                s->st.level_launches += s->cfg.max_levels;
+        for (SmallSlot &S : s->small)
+            if (S.busy) progress |= poll_small(s, S);
+        for (SmallSlot &S : s->small)
+            if (!S.busy && !s->pend_small.empty()) progress |= launch_small(s, S);
+        // large paths
+        const size_t mid_reserve =
+            std::min(s->arena.capacity() / 4, 32 * LevelEngine::footprint(kMidMaxN));
+        for (int e = 0; e < 2; ++e) {
+            LevelEngine &E = e == 0 ? s->mid : s->big;
+            std::deque<Request> &pend = e == 0 ? s->pend_mid : s->pend_big;
+            if (E.launched() && E.ready()) {
+                fin.clear();
+                E.collect(fin);
+                for (auto &f : fin) {
+                    auto it = s->large.find(f.tag);
+                    if (it == s->large.end()) continue;
+                    complete(s, it->second, f.state == kSlotDone ? SBFS_OK : SBFS_ECUDA, f.len, f.word);
+                    s->large.erase(it);
+                }
                 progress = true;
+            }
+            if (!E.launched()) {
+                while (!pend.empty()) {
+                    const Request &r = pend.front();
+                    if (e == 1 && E.in_flight() > 0 &&
+                        s->arena.used() + LevelEngine::footprint(r.n) + mid_reserve > s->arena.capacity())
+                        break;
+                    if (E.admit(nullptr, 32, r.n, (long long)r.id, r.a, r.b) < 0) break;
+                    s->large.emplace((long long)r.id, r);
+                    pend.pop_front();
+                }
+                if (E.in_flight() > 0) {
+                    E.launch(s->cfg.max_levels, none, 4 * s->cfg.max_levels);
+                    std::lock_guard<std::mutex> lock(s->mu);
+                    s->st.level_launches += s->cfg.max_levels;
+                    progress = true;
+                }
             }
         }
         {
             std::lock_guard<std::mutex> lock(s->mu);
             if (s->reset_peak) {
-                s->level.reset_peak();
+                s->arena.reset_peak();
                 s->reset_peak = false;
             }
-            s->st.pending = (int64_t)(s->incoming.size() + s->pend_small.size() + s->pend_large.size());
-            s->st.in_flight = (int64_t)(s->small_batch.size() + s->large.size());
-            s->st.arena_used = (int64_t)s->level.arena_used();
-            s->st.arena_peak = (int64_t)s->level.arena_peak();
-            s->st.arena_capacity = (int64_t)s->level.arena_capacity();
+            s->st.pending = (int64_t)(s->incoming.size() + s->pend_small.size() + s->pend_mid.size() +
+                                      s->pend_big.size());
+            size_t small_left = 0;
+            for (const SmallSlot &S : s->small) small_left += S.busy ? S.left : 0;
+            s->st.in_flight = (int64_t)(small_left + s->large.size());
+            s->st.arena_used = (int64_t)s->arena.used();
+            s->st.arena_peak = (int64_t)s->arena.peak();
+            s->st.arena_capacity = (int64_t)s->arena.capacity();
         }
         if (!progress) std::this_thread::sleep_for(std::chrono::microseconds(20));
     }
@@ -270,7 +326,8 @@ sbfs_status sbfs_server_start(const sbfs_server_config *cfg, sbfs_server **out)
     sbfs_config hc;
     sbfs_config_default(&hc);
     hc.device = s->cfg.device;
-    hc.streams = 2;
+    // small batches, n <= 20 level slots, n >= 21 level slots: stream priority in that order
+    hc.streams = kSmallSlots + 2;
     sbfs_status st = sbfs_create(&hc, &s->h);
     if (st) {
         delete s;
@@ -278,12 +335,31 @@ sbfs_status sbfs_server_start(const sbfs_server_config *cfg, sbfs_server **out)
     }
     const size_t mb = (size_t)s->cfg.max_batch;
     cudaError_t e = cudaSuccess;
-    if ((e = s->d_recs.reserve(mb * 64)) || (e = s->d_ns.reserve(mb)) || (e = s->d_len.reserve(mb * 4)) ||
-        (e = s->d_words.reserve(mb * kWords * 8)) || (e = s->h_recs.reserve(mb * 64)) || (e = s->h_ns.reserve(mb)) ||
-        (e = s->h_len.reserve(mb * 4)) || (e = s->h_words.reserve(mb * kWords * 8)) ||
-        (e = cudaEventCreateWithFlags(&s->small_ev, cudaEventDisableTiming)) ||
-        (e = s->level.init(s->h->sm_count, (size_t)s->cfg.arena_bytes, s->h->lanes[1].stream))) {
+    for (int i = 0; i < kSmallSlots && e == cudaSuccess; ++i) {
+        SmallSlot &S = s->small[i];
+        S.lane = i;
+        if ((e = S.d_recs.reserve(mb * 64)) || (e = S.d_ns.reserve(mb)) || (e = S.h_recs.reserve(mb * 64)) ||
+            (e = S.h_ns.reserve(mb)) || (e = S.h_len.reserve(mb * 4)) || (e = S.h_words.reserve(mb * kWords * 8)) ||
+            (e = S.h_flags.reserve(mb * 4)) || (e = cudaHostGetDevicePointer((void **)&S.dl, S.h_len.ptr, 0)) ||
+            (e = cudaHostGetDevicePointer((void **)&S.dw, S.h_words.ptr, 0)) ||
+            (e = cudaHostGetDevicePointer((void **)&S.df, S.h_flags.ptr, 0)) ||
+            (e = cudaEventCreateWithFlags(&S.ev, cudaEventDisableTiming)))
+            break;
+        std::memset(S.h_flags.ptr, 0, mb * 4);
+    }
+    if (e == cudaSuccess && (e = s->arena.reserve((size_t)s->cfg.arena_bytes)) == cudaSuccess &&
+        (e = s->mid.init(s->h->sm_count, 0, s->h->lanes[kSmallSlots].stream, &s->arena)) == cudaSuccess)
+        e = s->big.init(s->h->sm_count, 0, s->h->lanes[kSmallSlots + 1].stream, &s->arena);
+    if (e != cudaSuccess) {
         cudaGetLastError();
+        s->mid.destroy();
+        s->big.destroy();
+        s->arena.release();
+        for (SmallSlot &S : s->small) {
+            if (S.ev) cudaEventDestroy(S.ev);
+            for (DevBuf *d : {&S.d_recs, &S.d_ns}) d->release();
+            for (HostBuf *b : {&S.h_recs, &S.h_ns, &S.h_len, &S.h_words, &S.h_flags}) b->release();
+        }
         sbfs_destroy(s->h);
         delete s;
         return e == cudaErrorMemoryAllocation ? SBFS_ENOMEM : SBFS_ECUDA;
@@ -377,11 +453,16 @@ sbfs_status sbfs_server_stop(sbfs_server *s)
     s->cv_in.notify_all();
     if (s->loop.joinable()) s->loop.join();
     cudaSetDevice(s->h->device);
-    if (s->h->lanes.size() > 1) cudaStreamSynchronize(s->h->lanes[1].stream);
-    s->level.destroy();
-    if (s->small_ev) cudaEventDestroy(s->small_ev);
-    for (DevBuf *d : {&s->d_recs, &s->d_ns, &s->d_len, &s->d_words}) d->release();
-    for (HostBuf *b : {&s->h_recs, &s->h_ns, &s->h_len, &s->h_words}) b->release();
+    for (size_t i = 1; i < s->h->lanes.size(); ++i) cudaStreamSynchronize(s->h->lanes[i].stream);
+    cudaStreamSynchronize(s->h->lanes[0].stream);
+    s->mid.destroy();
+    s->big.destroy();
+    s->arena.release();
+    for (SmallSlot &S : s->small) {
+        if (S.ev) cudaEventDestroy(S.ev);
+        for (DevBuf *d : {&S.d_recs, &S.d_ns}) d->release();
+        for (HostBuf *b : {&S.h_recs, &S.h_ns, &S.h_len, &S.h_words, &S.h_flags}) b->release();
+    }
     sbfs_destroy(s->h);
     delete s;
     return SBFS_OK;
