@@ -18,13 +18,18 @@
 // Because state persists, the host (batch path or the serving loop) can admit
 // new automata into free slots between launches and launch levels back to
 // back (or from a CUDA graph) without waiting for the slowest automaton.
+#include <cooperative_groups.h>
+
 #include "level.cuh"
 
 namespace sbfs {
 namespace {
 
+namespace cg = cooperative_groups;
+
 constexpr int kThreads = 512;
 constexpr int kStage = 2 * kThreads;   // staged pushes per CTA round
+constexpr int kNarrowCluster = 8;      // CTAs of the narrow-level kernel's cluster
 
 struct LevelSmem {
     unsigned long long prefix[kMaxLevelSlots + 1];
@@ -35,6 +40,9 @@ struct LevelSmem {
     unsigned int slot_count[kMaxLevelSlots];
     unsigned long long slot_base[kMaxLevelSlots];
     unsigned long long warp_sum[kThreads / 32];
+    unsigned long long lvl_start[kMaxLevelSlots];   // current level's first queue index per slot
+    unsigned long long b_total;                     // narrow kernel: rank 0's transition results
+    int b_running;
     bool last;
 };
 
@@ -80,7 +88,7 @@ __device__ unsigned long long level_items(LevelSlot *slots, const uint64_t *tabl
         if (have) {
             s = find_slot(sh.prefix, nslots, item);
             sl = &slots[s];
-            idx = sl->lvl_start + (item - sh.prefix[s]);
+            idx = sh.lvl_start[s] + (item - sh.prefix[s]);
             const uint32_t x = (uint32_t)(__ldcg(sl->queue + idx) & kLevelSubsetMask);
             const uint64_t *tb = tables + (size_t)s * kLevelTable;
             t = __ldg(tb + (x & 255u));
@@ -296,6 +304,7 @@ __global__ void __launch_bounds__(kThreads) k_level(LevelSlot *slots, uint64_t *
         }
     }
     if (tid < kMaxLevelSlots) sh.slot_count[tid] = 0;
+    for (int q = tid; q < nslots; q += blockDim.x) sh.lvl_start[q] = slots[q].lvl_start;
     __syncthreads();
 
     unsigned long long expanded = level_items(slots, tables, sh, nslots, total, blockIdx.x, need);
@@ -323,33 +332,60 @@ __global__ void __launch_bounds__(kThreads) k_level(LevelSlot *slots, uint64_t *
     }
 }
 
-// Narrow levels: one CTA runs consecutive levels by itself -- expand, move to
-// the next level, repeat -- while the levels stay at most `narrow` subsets
-// wide, up to `max_levels` levels, with no launch or grid barrier in between.
-// It is launched as a grid of one CTA, and only when no slot awaits set-up.
-__global__ void __launch_bounds__(kThreads) k_level_narrow(LevelSlot *slots, uint64_t *tables, LevelCtl *ctl,
-                                                           Batch out, int par, int max_levels,
-                                                           unsigned long long narrow)
+// Narrow levels: one cluster of kNarrowCluster CTAs runs consecutive levels by
+// itself -- all CTAs expand their share of the level, rank 0 moves every slot
+// to its next level, the others take the new prefix sums from rank 0's shared
+// memory -- with hardware cluster barriers instead of launches between levels,
+// while the levels stay at most `narrow` subsets wide, up to `max_levels`
+// levels.  Launched as one cluster, and only when no slot awaits set-up.
+__global__ void __cluster_dims__(kNarrowCluster, 1, 1) __launch_bounds__(kThreads)
+    k_level_narrow(LevelSlot *slots, uint64_t *tables, LevelCtl *ctl, Batch out, int par, int max_levels,
+                   unsigned long long narrow)
 {
     __shared__ LevelSmem sh;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank();
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int nslots = ctl->nslots;
     unsigned long long total = ctl->total[par];
     const int pn = min(ctl->prefix_n[par], nslots);
     for (int i = tid; i <= nslots; i += blockDim.x) sh.prefix[i] = ctl->prefix[par][i <= pn ? i : pn];
+    for (int q = tid; q < nslots; q += blockDim.x) sh.lvl_start[q] = slots[q].lvl_start;
     if (tid < kMaxLevelSlots) sh.slot_count[tid] = 0;
     __syncthreads();
     unsigned long long expanded = 0;
     int running = 0;
+    LevelSmem *sh0 = cluster.map_shared_rank(&sh, 0);
     for (int it = 0; it < max_levels; ++it) {
-        expanded += level_items(slots, tables, sh, nslots, total, 0, 1);
-        __syncthreads();
-        total = level_transition(slots, ctl, out, sh, nslots, sh.prefix, running);
+        expanded += level_items(slots, tables, sh, nslots, total, rank, kNarrowCluster);
+        cluster.sync();   // every CTA's pushes of this level are in
+        if (rank == 0) {
+            total = level_transition(slots, ctl, out, sh, nslots, sh.prefix, running);
+            if (tid == 0) {
+                sh.b_total = total;
+                sh.b_running = running;
+            }
+            for (int q = tid; q < nslots; q += blockDim.x) sh.lvl_start[q] = slots[q].lvl_start;
+        }
+        cluster.sync();   // rank 0's transition is visible
+        if (rank != 0) {
+            for (int i = tid; i <= nslots; i += blockDim.x) sh.prefix[i] = sh0->prefix[i];
+            for (int q = tid; q < nslots; q += blockDim.x) sh.lvl_start[q] = sh0->lvl_start[q];
+            total = sh0->b_total;
+            running = sh0->b_running;
+            __syncthreads();
+        } else {
+            __syncthreads();
+            total = sh.b_total;
+            running = sh.b_running;
+        }
         if (running == 0 || total > narrow) break;
     }
     for (int o = 16; o; o >>= 1) expanded += __shfl_down_sync(kFull, expanded, o);
     if (lane == 0 && expanded) atomicAdd(&ctl->expanded, expanded);
+    cluster.sync();   // rank 0's shared memory stays valid until every CTA is done reading it
+    if (rank != 0) return;
     const int nxt = par ^ 1;
     for (int i = tid; i <= nslots; i += blockDim.x) ctl->prefix[nxt][i] = sh.prefix[i];
     if (tid == 0) {
@@ -386,7 +422,7 @@ cudaError_t launch_level_narrow(int parity, int max_levels, unsigned long long n
                                 uint64_t *tables, LevelCtl *ctl, const Batch &out, cudaStream_t st)
 {
     if (max_levels < 1) return cudaErrorInvalidValue;
-    k_level_narrow<<<1, kThreads, 0, st>>>(slots, tables, ctl, out, parity & 1, max_levels, narrow);
+    k_level_narrow<<<kNarrowCluster, kThreads, 0, st>>>(slots, tables, ctl, out, parity & 1, max_levels, narrow);
     return cudaGetLastError();
 }
 

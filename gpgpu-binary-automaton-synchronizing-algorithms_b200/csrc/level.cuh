@@ -62,8 +62,9 @@ cudaError_t launch_level(int ctas, int parity, LevelSlot *slots, uint64_t *table
 cudaError_t launch_level_narrow(int parity, int max_levels, unsigned long long narrow, LevelSlot *slots,
                                 uint64_t *tables, LevelCtl *ctl, const Batch &out, cudaStream_t st);
 
-// Level totals at or below this are expanded by one CTA looping over levels.
-constexpr unsigned long long kNarrowLevel = 4096;
+// Level totals at or below this are expanded by one cluster of CTAs looping
+// over levels (k_level_narrow).
+constexpr unsigned long long kNarrowLevel = 16384;
 
 // First-fit allocator over one device buffer (host-side bookkeeping only).
 class Arena {
