@@ -15,10 +15,13 @@
 // entry carries the letters of the word that reaches it (bit NMAX + d =
 // letter d, 1 = b), so a word needs no parent pointers or retained history.
 //
-// Each iteration a lane takes up to two subsets of its current level and looks
-// up their four images.  A singleton among them ends the search (no singleton
+// Each iteration a lane takes up to kStep (4) subsets of its current level and
+// looks up their eight images: more independent work per step hides the
+// shared-memory latencies that one warp's dependent chain exposes at 7 warps
+// per SM (2 -> 4 subsets: 0.64 -> 0.56 ms per 10^6 automata at n = 12; 6 and 8
+// were slower again).  A singleton among them ends the search (no singleton
 // is visited before the first one is generated, so it needs no bitmap test).
-// Otherwise the four images are test-and-set with shared-memory atomicOr, issued
+// Otherwise the eight images are test-and-set with shared-memory atomicOr, issued
 // back to back and kept in program order by the hardware for a repeated
 // address, and the fresh ones are appended in queue order (first subset's a, b,
 // then the second's), as the sequential loop would.
@@ -46,6 +49,7 @@ namespace sbfs {
 namespace {
 
 constexpr int kActive = 0, kDone = 1, kEscalate = 2, kIdle = 3, kHeld = 4;
+constexpr int kStep = 4;   // subsets a lane expands per step (their 2 * kStep images are tested together)
 
 __host__ __device__ constexpr int low_bit4(int v)
 {
@@ -426,43 +430,55 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
             }
         }
 
-        // ---- up to two expansions per active lane ----------------------------
+        // ---- up to kStep expansions per active lane ----------------------------
         if (state == kActive) {
-            // a lane with one subset left in the level expands it twice: the
-            // second copy's images are already visited by the time they are tested
-            const bool two = head + 1u < lvl_end;
-            const uint32_t e0 = rq[(head & rmask) * 32];
-            const uint32_t e1 = two ? rq[((head + 1u) & rmask) * 32] : e0;
-            head += two ? 2u : 1u;
-            expanded += two ? 2u : 1u;
-            const uint32_t t0 = lane_image<NMAX>(tb, e0 & G::kMask);
-            const uint32_t t1 = lane_image<NMAX>(tb, e1 & G::kMask);
-            const uint32_t y[4] = {t0 >> 16, t0 & 0xFFFFu, t1 >> 16, t1 & 0xFFFFu};
+            // a lane with fewer than kStep subsets left in the level expands its
+            // first one again in the spare places: those copies' images are
+            // already visited by the time they are tested
+            constexpr int P = kStep;
+            const uint32_t take = min(lvl_end - head, (uint32_t)P);
+            uint32_t e[P];
+#pragma unroll
+            for (int i = 0; i < P; ++i)
+                e[i] = (i == 0 || (uint32_t)i < take) ? rq[((head + (uint32_t)i) & rmask) * 32] : e[0];
+            head += take;
+            expanded += take;
+            uint32_t y[2 * P], hi[2 * P];
             // entries carry the word that reaches them: the parent's letters,
             // plus letter `level` = b for the b-images (an entry holds 32 - NMAX
             // letters; at level >= 32 - NMAX a fresh image escalates instead)
             const uint32_t lb = (WORDS && level < (uint32_t)G::kWordMax) ? 1u << (level + NMAX) : 0u;
-            const uint32_t hi[4] = {WORDS ? (e0 & ~G::kMask) : 0u, WORDS ? ((e0 & ~G::kMask) | lb) : 0u,
-                                    WORDS ? (e1 & ~G::kMask) : 0u, WORDS ? ((e1 & ~G::kMask) | lb) : 0u};
+#pragma unroll
+            for (int i = 0; i < P; ++i) {
+                const uint32_t t = lane_image<NMAX>(tb, e[i] & G::kMask);
+                y[2 * i] = t >> 16;
+                y[2 * i + 1] = t & 0xFFFFu;
+                hi[2 * i] = WORDS ? (e[i] & ~G::kMask) : 0u;
+                hi[2 * i + 1] = WORDS ? ((e[i] & ~G::kMask) | lb) : 0u;
+            }
             // no singleton is ever visited (the search stops at the first one), so
             // a singleton image ends the search without a bitmap test
             int sc = -1;
 #pragma unroll
-            for (int c = 3; c >= 0; --c)
+            for (int c = 2 * P - 1; c >= 0; --c)
                 if (is_singleton(y[c])) sc = c;
             if (sc >= 0) {
                 state = kDone;
                 res_len = (int32_t)level + 1;
-                res_word = WORDS ? (((sc < 2 ? e0 : e1) >> NMAX) | ((uint32_t)(sc & 1) << level)) : 0u;
+                uint32_t es = e[0];
+#pragma unroll
+                for (int i = 1; i < P; ++i)
+                    if ((sc >> 1) == i) es = e[i];
+                res_word = WORDS ? ((es >> NMAX) | ((uint32_t)(sc & 1) << level)) : 0u;
             } else {
                 // test-and-set in queue order: a subset met twice in this step is
                 // fresh only the first time (same-address atomics keep program order)
-                uint32_t old[4];
+                uint32_t old[2 * P];
 #pragma unroll
-                for (int c = 0; c < 4; ++c) old[c] = atomicOr(&bm[(y[c] >> 5) * 32], 1u << (y[c] & 31u));
+                for (int c = 0; c < 2 * P; ++c) old[c] = atomicOr(&bm[(y[c] >> 5) * 32], 1u << (y[c] & 31u));
                 bool any = false;
 #pragma unroll
-                for (int c = 0; c < 4; ++c) {
+                for (int c = 0; c < 2 * P; ++c) {
                     if (!(old[c] & (1u << (y[c] & 31u)))) {
                         rq[(tail & rmask) * 32] = y[c] | hi[c];
                         ++tail;
@@ -470,7 +486,7 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
                     }
                 }
                 // more live entries than ring slots (the oldest were overwritten), or
-                // a word longer than an entry carries: the pooled kernel takes over
+                // a word longer than an entry carries: the whole-warp search takes over
                 if (tail - head > (uint32_t)ring || (WORDS && any && level >= (uint32_t)G::kWordMax)) {
                     state = kEscalate;
                 } else if (head == lvl_end) {
