@@ -253,6 +253,9 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
 
     const int present = class_present_mask(j);
     const size_t escal_entries = (size_t)std::max<int64_t>(j.count, 1);
+    // a mixed batch: classes 0..2 each on their own stream, forked after the bucketing
+    const bool fork = j.ns && !plain && __builtin_popcount((unsigned)present) > 1 && L.aux[0];
+    bool joined[3] = {false, false, false};
     if (j.ns) {
         CK(L.order.reserve((size_t)j.count * sizeof(int32_t)), "allocating order array");
         // hist[K] | ranges[2K] | cursor[K]
@@ -262,25 +265,33 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
         CK(launch_classify(j.ns, j.count, sc, h->sm_count, st), "launching size-class bucketing");
         *launches += 3;
         b.order = sc.order;
+        if (fork) CK(cudaEventRecord(L.ev_fork, st), "recording event");
     }
     for (int c = 0; c < kNumClasses; ++c) {
         if (!(present & (1 << c))) continue;
         Batch bc = b;
         if (j.ns) bc.range_dev = L.ranges.as<unsigned long long>() + kNumClasses + 2 * c;
         unsigned long long *ticket = ticket_override ? ticket_override : &ctr->ticket[c];
+        cudaStream_t cs = st;
+        if (fork && c < 3) {
+            cs = L.aux[c];
+            CK(cudaStreamWaitEvent(cs, L.ev_fork, 0), "ordering streams");
+            joined[c] = true;
+        }
         if (c < 2 && !plain && !P.use_pool[c]) {
             const LaneShape &ls = P.lane[c];
             // one escalation list per lane class; entries read as -1 until stored
             CK(L.escal.reserve(2 * escal_entries * sizeof(int32_t)), "allocating escalation list");
             int32_t *list = L.escal.as<int32_t>() + (size_t)c * escal_entries;
-            CK(cudaMemsetAsync(list, 0xFF, escal_entries * sizeof(int32_t), st), "resetting escalation list");
+            CK(cudaMemsetAsync(list, 0xFF, escal_entries * sizeof(int32_t), cs), "resetting escalation list");
             CK(launch_lane(ls.nmax, ls.warps, ls.ring, ls.refill_k, ls.tail_k, ls.ctas, bc, list, escal_entries,
-                           &ctr->escal_count[c], &ctr->escal_claim[c], ticket, LaneStream{}, st),
+                           &ctr->escal_count[c], &ctr->escal_claim[c], ticket, LaneStream{}, cs),
                "launching per-lane kernel");
         } else if (c < 3) {
             const PoolShape &s = P.pool[c];
-            CK(L.spill.reserve(pool_spill_words(s) * sizeof(uint32_t)), "allocating queue spill");
-            CK(launch_pool(s, bc, L.spill.as<uint32_t>(), ticket, st), "launching small-n kernel");
+            DevBuf &spill = fork ? L.spill_c[c] : L.spill;
+            CK(spill.reserve(pool_spill_words(s) * sizeof(uint32_t)), "allocating queue spill");
+            CK(launch_pool(s, bc, spill.as<uint32_t>(), ticket, cs), "launching small-n kernel");
         } else if (c == 3 && P.class3_level && !plain) {
             sbfs_status ls = run_level_class(h, L, j, bc, launches);
             if (ls) return ls;
@@ -299,7 +310,10 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
             continue;
         }
         *launches += 1;
+        if (joined[c]) CK(cudaEventRecord(L.ev_join[c], cs), "recording event");
     }
+    for (int c = 0; c < 3; ++c)
+        if (joined[c]) CK(cudaStreamWaitEvent(st, L.ev_join[c], 0), "ordering streams");
     if (!plain && j.len && j.count > 0 && !j.done_flag) {
         CK(launch_count_sync(j.len, j.count, &ctr->synchronizing, h->sm_count, st), "launching result count");
         *launches += 1;
@@ -1024,10 +1038,17 @@ sbfs_status sbfs_create(const sbfs_config *cfg, sbfs_handle **out)
         if ((e = cudaStreamCreateWithPriority(&L.stream, cudaStreamNonBlocking, prio)) != cudaSuccess ||
             (e = cudaEventCreate(&L.ev_k0)) != cudaSuccess || (e = cudaEventCreate(&L.ev_k1)) != cudaSuccess ||
             (e = cudaEventCreateWithFlags(&L.ev_done, cudaEventDisableTiming)) != cudaSuccess ||
-            (e = cudaEventCreateWithFlags(&L.ev_in, cudaEventDisableTiming)) != cudaSuccess) {
+            (e = cudaEventCreateWithFlags(&L.ev_in, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&L.ev_fork, cudaEventDisableTiming)) != cudaSuccess) {
             sbfs_destroy(h);
             return cuda_fail(nullptr, e, "creating streams");
         }
+        for (int c = 0; c < 3; ++c)
+            if ((e = cudaStreamCreateWithPriority(&L.aux[c], cudaStreamNonBlocking, prio)) != cudaSuccess ||
+                (e = cudaEventCreateWithFlags(&L.ev_join[c], cudaEventDisableTiming)) != cudaSuccess) {
+                sbfs_destroy(h);
+                return cuda_fail(nullptr, e, "creating streams");
+            }
     }
     *out = h;
     return SBFS_OK;
@@ -1039,6 +1060,8 @@ sbfs_status sbfs_destroy(sbfs_handle *h)
     cudaSetDevice(h->device);
     for (auto &L : h->lanes) {
         if (L.stream) cudaStreamSynchronize(L.stream);
+        for (cudaStream_t a : L.aux)
+            if (a) cudaStreamSynchronize(a);
         L.drop_graphs();
         for (DevBuf *d : {&L.maps, &L.ns, &L.len, &L.words, &L.spill, &L.order, &L.counters, &L.ranges,
                           &L.cta_queue, &L.hbm_bitmap, &L.hbm_queue, &L.escal, &L.tickets})
@@ -1048,6 +1071,12 @@ sbfs_status sbfs_destroy(sbfs_handle *h)
         if (L.ev_k1) cudaEventDestroy(L.ev_k1);
         if (L.ev_done) cudaEventDestroy(L.ev_done);
         if (L.ev_in) cudaEventDestroy(L.ev_in);
+        if (L.ev_fork) cudaEventDestroy(L.ev_fork);
+        for (int c = 0; c < 3; ++c) {
+            if (L.aux[c]) cudaStreamDestroy(L.aux[c]);
+            if (L.ev_join[c]) cudaEventDestroy(L.ev_join[c]);
+            L.spill_c[c].release();
+        }
         if (L.level_ready) L.level.destroy();
         if (L.stream) cudaStreamDestroy(L.stream);
     }

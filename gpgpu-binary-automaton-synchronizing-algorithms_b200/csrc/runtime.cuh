@@ -83,6 +83,11 @@ struct Lane {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr, ev_done = nullptr;
     cudaEvent_t ev_in = nullptr;               // this lane's records have arrived (host path)
+    // a mixed batch's size classes 0..2 run on these, beside class 3 on `stream`
+    // (their tails -- a Cerny C_16 or C_20 each -- then overlap instead of adding up)
+    cudaStream_t aux[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_join[3] = {nullptr, nullptr, nullptr};
+    DevBuf spill_c[3];                         // queue spill of a pooled class, one per class
     DevBuf maps, ns, len, words, spill, order, counters, ranges, cta_queue, hbm_bitmap, hbm_queue,
         escal, tickets;
     LevelEngine level;                         // device-resident slots for n > 20
@@ -109,7 +114,7 @@ struct Lane {
     {
         uint64_t x = 1469598103934665603ull;
         for (const DevBuf *d : {&maps, &ns, &len, &words, &spill, &order, &counters, &ranges, &cta_queue, &escal,
-                                &tickets})
+                                &tickets, &spill_c[0], &spill_c[1], &spill_c[2]})
             x = (x ^ reinterpret_cast<uint64_t>(d->ptr)) * 1099511628211ull;
         for (const HostBuf *b : {&h_counters, &h_maps, &h_ns, &h_len, &h_words})
             x = (x ^ reinterpret_cast<uint64_t>(b->ptr)) * 1099511628211ull;
