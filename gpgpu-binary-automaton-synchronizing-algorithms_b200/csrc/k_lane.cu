@@ -142,7 +142,8 @@ __device__ void warp_solve(const Batch &b, int64_t k, uint32_t *region, int lane
         q[0] = full;
     }
     __syncwarp();
-    uint32_t head = 0, lvl_end = 1, tail = 1, level = 0;
+    // n = 1: the visited root is the only singleton (see the per-lane set-up)
+    uint32_t head = 0, lvl_end = n > 1 ? 1u : 0u, tail = lvl_end, level = 0;
     int32_t len = kLenNonSync;
     uint32_t found = 0, found_letter = 0;
     while (true) {
@@ -391,6 +392,15 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
                         state = kDone;
                         res_len = kLenInvalid;
                         res_word = 0;
+                    } else if (n == 1) {
+                        // the root is the only singleton and it is visited, so the
+                        // search never generates a new one: not synchronizing, as in
+                        // GPGPU/CPU/SlimCPUUntweaked.cs:149-157 (and the singleton-first
+                        // test below, which relies on no singleton being visited, is
+                        // never reached)
+                        state = kDone;
+                        res_len = kLenNonSync;
+                        res_word = 0;
                     } else {
 #pragma unroll 16
                         for (int w = 0; w < BW; ++w) bm[w * 32] = 0u;
@@ -414,6 +424,9 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
                 }
                 if (state == kHeld) state = kIdle;
                 if (!more) {
+                    // an outcome decided during set-up (n = 1, a malformed record) is
+                    // written by the next refill pass: take that pass before leaving
+                    if (__any_sync(kFull, state == kDone || state == kEscalate)) continue;
                     // no new automata either: solve escalated ones while any can be claimed
                     while (true) {
                         int64_t e = -1;

@@ -5,6 +5,8 @@ replays to a singleton and has the returned length; the Cerny bound (n-1)^2 is
 checked per automaton (Verify.cs:12-62).  Sizes follow the benchmark
 configurations with seeded synthetic inputs.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -325,3 +327,41 @@ def test_streamed_path_violation_and_malformed(oracle_mod):
         assert ei.value.status == 1
         r = eng.solve(recs, n=12, lstride=12)   # the handle stays usable
         assert r["first_violation"] == -1 and r["len"][333_333] == 121
+
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "small_automata.npz")
+
+
+def test_golden_fixtures_on_every_small_path(engine):
+    """The committed fixtures (lengths from word enumeration, not from a BFS):
+    n = 2 and 3 exhaustive, n = 4..6 seeded; per-lane, warp-pooled and plain."""
+    d = np.load(GOLDEN)
+    recs, ns, lens = d["recs"], d["ns"], d["lens"]
+    np.testing.assert_array_equal(engine.solve(recs, ns=ns)["len"], lens)
+    with sbfs.Engine(device=0, small_kernel=2) as pooled:
+        np.testing.assert_array_equal(pooled.solve(recs, ns=ns)["len"], lens)
+    few = slice(0, None, 40)
+    np.testing.assert_array_equal(engine.solve(recs[few], ns=ns[few], plain=True)["len"], lens[few])
+
+
+def test_one_state_automata_match_the_oracle(engine, oracle_mod):
+    recs = np.zeros((4, 64), dtype=np.uint8)   # n = 1: both letters map state 0 to itself
+    r = engine.solve(recs, n=1)
+    ref = oracle_mod.solve(recs, n=1, words=False)
+    np.testing.assert_array_equal(r["len"], ref["len"])
+
+
+def test_largest_sizes(engine, oracle_mod):
+    """n = 25..28 (2^28-bit bitmaps in the level slots), the Cerny automaton at
+    the maximum size, and a slowly synchronizing permutation + merge."""
+    ns = np.array([25, 26, 27, 28, 28, 28, 24], dtype=np.uint8)
+    rows = [P.uniform_maps(1, int(n), 900 + i)[0] for i, n in enumerate(ns[:-3])]
+    rows += [P.cerny_record(28), P.uniform_maps(1, 28, 999)[0], P.perm_merge_record(24, 7)]
+    recs = np.stack(rows)
+    r = engine.solve(recs, ns=ns)
+    assert r["len"][4] == 27 * 27
+    check = [0, 1, 2, 3, 5, 6]
+    ref = oracle_mod.solve(recs[check], ns=ns[check], words=False, threads=8)
+    np.testing.assert_array_equal(r["len"][check], ref["len"])
+    assert oracle_mod.replay(recs, r["len"], r["words"], ns=ns)[0] == 0
+    assert r["first_violation"] == -1
