@@ -36,6 +36,21 @@ __global__ void k_gen(uint8_t *recs, int lstride, int n, int64_t count, unsigned
     }
 }
 
+// Overwrites every `every`-th record with the Cerny automaton C_n (a: i -> i+1
+// mod n, b: 0 -> 1, others fixed; length (n-1)^2): the heavy members the
+// benchmark configurations mix in (1 % to 5 %).
+__global__ void k_gen_cerny(uint8_t *recs, int lstride, int n, int64_t count, int every)
+{
+    for (int64_t k = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) * every; k < count;
+         k += (int64_t)gridDim.x * blockDim.x * every) {
+        uint8_t *rec = recs + (size_t)k * 2 * lstride;
+        for (int j = 0; j < n; ++j) {
+            rec[j] = (uint8_t)((j + 1) % n);
+            rec[lstride + j] = (uint8_t)(j == 0 ? 1 : j);
+        }
+    }
+}
+
 struct Bench {
     sbfs_handle *h;
     Lane *L;
@@ -43,13 +58,14 @@ struct Bench {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
 };
 
-cudaError_t prepare(Bench &b, int n, int64_t count)
+cudaError_t prepare(Bench &b, int n, int64_t count, int cerny_every = 0)
 {
     cudaError_t e;
     if ((e = b.recs.reserve((size_t)count * 64)) != cudaSuccess) return e;
     if ((e = b.len.reserve((size_t)count * 4)) != cudaSuccess) return e;
     if ((e = b.words.reserve((size_t)count * 8 * 6)) != cudaSuccess) return e;
     k_gen<<<1024, 256, 0, b.L->stream>>>(b.recs.as<uint8_t>(), 32, n, count, 0x5EEDull + (unsigned)n);
+    if (cerny_every > 0) k_gen_cerny<<<64, 128, 0, b.L->stream>>>(b.recs.as<uint8_t>(), 32, n, count, cerny_every);
     return cudaGetLastError();
 }
 
@@ -80,7 +96,7 @@ std::string device_key(sbfs_handle *h)
     cudaDeviceProp p;
     cudaGetDeviceProperties(&p, h->device);
     char buf[320];
-    std::snprintf(buf, sizeof buf, "%s|sm%d|abi%d|v7", p.name, h->sm_count, SBFS_ABI_VERSION);
+    std::snprintf(buf, sizeof buf, "%s|sm%d|abi%d|v8", p.name, h->sm_count, SBFS_ABI_VERSION);
     for (char *c = buf; *c; ++c)
         if (*c == ' ') *c = '_';
     return buf;
@@ -261,7 +277,9 @@ cudaError_t plan_autotune(sbfs_handle *h, Plan &plan)
         P.pool[2] = best.pool[2];
     }
     // ---- class 3: shared-memory bitmaps (per CTA) vs HBM bitmaps (level slots)
-    if (e == cudaSuccess && (e = prepare(b, 20, 1 << 13)) == cudaSuccess) {
+    // (2 % Cerny C_20 in the batch: their long thin searches set a class-3
+    // launch's makespan in the mixed and serving configurations)
+    if (e == cudaSuccess && (e = prepare(b, 20, 1 << 13, 50)) == cudaSuccess) {
         Plan best = P;
         double best_ms = 1e30;
         for (int threads : {256, 512, 1024}) {
