@@ -90,6 +90,10 @@ __global__ void finalize_violation(const DevCounters *c, int64_t *out)
 thread_local std::string g_create_error;
 
 constexpr int kDefaultLanes = 4;
+// levels a pooled warp spends on one automaton before handing it to the
+// CTA-wide kernel: random automata with n <= 20 stay below 40 (max 36 in 20K
+// samples at n = 20), a Cerny automaton needs (n-1)^2
+constexpr int kPoolLevelCap = 48;
 constexpr int64_t kDefaultChunk = 1 << 18;
 
 sbfs_status fail(sbfs_handle *h, sbfs_status st, const std::string &msg)
@@ -291,7 +295,26 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
             const PoolShape &s = P.pool[c];
             DevBuf &spill = fork ? L.spill_c[c] : L.spill;
             CK(spill.reserve(pool_spill_words(s) * sizeof(uint32_t)), "allocating queue spill");
-            CK(launch_pool(s, bc, spill.as<uint32_t>(), ticket, cs), "launching small-n kernel");
+            if (plain || ticket_override) {
+                CK(launch_pool(s, bc, spill.as<uint32_t>(), ticket, cs), "launching small-n kernel");
+            } else {
+                // long thin searches (Cerny automata: (n-1)^2 levels) leave the pooled
+                // warp after kPoolLevelCap levels for the CTA-wide kernel, same stream
+                CK(L.heavy[c].reserve(escal_entries * sizeof(int32_t)), "allocating hand-off list");
+                PoolHeavy hv{kPoolLevelCap, L.heavy[c].as<int32_t>(), &ctr->heavy_range[c][1]};
+                CK(launch_pool(s, bc, spill.as<uint32_t>(), ticket, cs, hv), "launching small-n kernel");
+                Batch bh = bc;
+                bh.order = L.heavy[c].as<int32_t>();
+                bh.range_dev = ctr->heavy_range[c];
+                const int nb = s.nmax;
+                const int per_sm = cta_max_ctas_per_sm(nb, P.cta.threads);
+                if (per_sm < 1) return fail(h, SBFS_ECUDA, "hand-off kernel does not fit on an SM");
+                const int ctas = std::min(P.cta.ctas, per_sm * h->sm_count);
+                CK(L.heavy_queue[c].reserve(cta_queue_entries(nb, ctas) * sizeof(uint64_t)), "allocating CTA queues");
+                CK(launch_cta(nb, P.cta.threads, ctas, bh, L.heavy_queue[c].as<uint64_t>(), &ctr->heavy_ticket[c], cs),
+                   "launching hand-off kernel");
+                *launches += 1;
+            }
         } else if (c == 3 && P.class3_level && !plain) {
             sbfs_status ls = run_level_class(h, L, j, bc, launches);
             if (ls) return ls;
@@ -310,7 +333,7 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
             continue;
         }
         *launches += 1;
-        if (joined[c]) CK(cudaEventRecord(L.ev_join[c], cs), "recording event");
+        if (c < 3 && joined[c]) CK(cudaEventRecord(L.ev_join[c], cs), "recording event");
     }
     for (int c = 0; c < 3; ++c)
         if (joined[c]) CK(cudaStreamWaitEvent(st, L.ev_join[c], 0), "ordering streams");

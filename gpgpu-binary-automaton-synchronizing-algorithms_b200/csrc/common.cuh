@@ -105,8 +105,17 @@ struct PoolShape {
 
 size_t pool_smem_bytes(const PoolShape &s);
 size_t pool_spill_words(const PoolShape &s);   // uint32 spill words for the whole grid
+// Optional hand-off of long searches: a slot that reaches level_cap levels is
+// abandoned and its automaton appended to list (count = entries appended), to
+// be solved by a kernel with more threads per automaton.  list == nullptr = off.
+struct PoolHeavy {
+    int level_cap;
+    int32_t *list;
+    unsigned long long *count;
+};
 cudaError_t launch_pool(const PoolShape &s, const Batch &b, uint32_t *spill,
-                        unsigned long long *ticket, cudaStream_t st);
+                        unsigned long long *ticket, cudaStream_t st, const PoolHeavy &heavy = PoolHeavy{0, nullptr,
+                                                                                                        nullptr});
 int pool_max_ctas_per_sm(const PoolShape &s);
 
 size_t lane_smem_bytes(int nmax, int warps, int ring);

@@ -54,7 +54,7 @@ __device__ __forceinline__ uint32_t table_image(const uint32_t *tb, uint32_t x)
 
 template <int NMAX, int S>
 __global__ void __launch_bounds__(512) k_pool(Batch b, int q_smem, int grab, uint32_t *spill,
-                                              unsigned long long *ticket)
+                                              unsigned long long *ticket, PoolHeavy heavy)
 {
     using G = PoolGeom<NMAX>;
     constexpr int BW = G::kBitmapWords;
@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(512) k_pool(Batch b, int q_smem, int grab, uin
         // ---- per-slot bookkeeping (owner lanes) -----------------------------
         const unsigned fa = __ballot_sync(kFull, fnd0);
         const unsigned fb = __ballot_sync(kFull, fnd1);
-        bool done = false;
+        bool done = false, esc = false;
         int32_t res_len = kLenNonSync;
         uint32_t f_parent = 0, f_letter = 0;
         const unsigned fr = (fa | fb) & own_range;
@@ -259,9 +259,21 @@ __global__ void __launch_bounds__(512) k_pool(Batch b, int q_smem, int grab, uin
             } else {
                 my_lvl_end = my_tail;
                 ++my_level;
+                // a long thin search (a Cerny automaton has (n-1)^2 levels; random
+                // ones here stay far below the cap) goes to a CTA-wide kernel
+                if (heavy.list && my_level >= (uint32_t)heavy.level_cap) esc = true;
             }
         }
         __syncwarp();
+
+        const unsigned em = __ballot_sync(kFull, esc);
+        if (em) {
+            unsigned long long pos = 0;
+            const int leader = __ffs(em) - 1;
+            if (lane == leader) pos = atomicAdd(heavy.count, (unsigned long long)__popc(em));
+            pos = __shfl_sync(kFull, pos, leader);
+            if (esc) heavy.list[pos + __popc(em & ((1u << lane) - 1u))] = (int32_t)my_k;
+        }
 
         // ---- finished slots: result, word, bitmap clear ---------------------
         if (done) {
@@ -295,7 +307,7 @@ __global__ void __launch_bounds__(512) k_pool(Batch b, int q_smem, int grab, uin
             }
             publish_result(b, my_k);
         }
-        unsigned done_mask = __ballot_sync(kFull, done);
+        unsigned done_mask = __ballot_sync(kFull, done || esc);
         while (done_mask) {
             const int s = __ffs(done_mask) - 1;
             done_mask &= done_mask - 1;
@@ -312,7 +324,7 @@ __global__ void __launch_bounds__(512) k_pool(Batch b, int q_smem, int grab, uin
                 for (uint32_t i = lane; i < tail; i += 32) bm[(qload(s, i) & 0xFFFFu) >> 5] = 0u;
             }
         }
-        if (done) my_active = 0;
+        if (done || esc) my_active = 0;
         __syncwarp();
     }
     if (lane == 0 && b.expanded) atomicAdd(b.expanded, expanded);
@@ -320,25 +332,26 @@ __global__ void __launch_bounds__(512) k_pool(Batch b, int q_smem, int grab, uin
 
 template <int NMAX, int S>
 cudaError_t launch_t(const PoolShape &s, const Batch &b, uint32_t *spill,
-                     unsigned long long *ticket, cudaStream_t st)
+                     unsigned long long *ticket, cudaStream_t st, const PoolHeavy &hv)
 {
     const size_t smem = pool_smem_bytes(s);
     cudaError_t e = cudaFuncSetAttribute(k_pool<NMAX, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    k_pool<NMAX, S><<<s.ctas, s.warps * 32, smem, st>>>(b, s.queue_smem, s.grab > 0 ? s.grab : 16, spill, ticket);
+    k_pool<NMAX, S><<<s.ctas, s.warps * 32, smem, st>>>(b, s.queue_smem, s.grab > 0 ? s.grab : 16, spill, ticket,
+                                                         hv);
     return cudaGetLastError();
 }
 
 template <int NMAX>
 cudaError_t launch_n(const PoolShape &s, const Batch &b, uint32_t *spill,
-                     unsigned long long *ticket, cudaStream_t st)
+                     unsigned long long *ticket, cudaStream_t st, const PoolHeavy &hv)
 {
     switch (s.slots) {
-    case 4: return launch_t<NMAX, 4>(s, b, spill, ticket, st);
-    case 8: return launch_t<NMAX, 8>(s, b, spill, ticket, st);
-    case 16: return launch_t<NMAX, 16>(s, b, spill, ticket, st);
-    case 32: return launch_t<NMAX, 32>(s, b, spill, ticket, st);
+    case 4: return launch_t<NMAX, 4>(s, b, spill, ticket, st, hv);
+    case 8: return launch_t<NMAX, 8>(s, b, spill, ticket, st, hv);
+    case 16: return launch_t<NMAX, 16>(s, b, spill, ticket, st, hv);
+    case 32: return launch_t<NMAX, 32>(s, b, spill, ticket, st, hv);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -400,13 +413,14 @@ int pool_max_ctas_per_sm(const PoolShape &s)
 }
 
 cudaError_t launch_pool(const PoolShape &s, const Batch &b, uint32_t *spill,
-                        unsigned long long *ticket, cudaStream_t st)
+                        unsigned long long *ticket, cudaStream_t st, const PoolHeavy &heavy)
 {
     if (s.queue_smem < 32 || s.warps < 1 || s.warps > 16 || s.ctas < 1) return cudaErrorInvalidValue;
+    if (heavy.list && (heavy.level_cap < 1 || !heavy.count)) return cudaErrorInvalidValue;
     switch (s.nmax) {
-    case 8: return launch_n<8>(s, b, spill, ticket, st);
-    case 12: return launch_n<12>(s, b, spill, ticket, st);
-    case 16: return launch_n<16>(s, b, spill, ticket, st);
+    case 8: return launch_n<8>(s, b, spill, ticket, st, heavy);
+    case 12: return launch_n<12>(s, b, spill, ticket, st, heavy);
+    case 16: return launch_n<16>(s, b, spill, ticket, st, heavy);
     default: return cudaErrorInvalidValue;
     }
 }
