@@ -393,7 +393,7 @@ sbfs_status ensure_plan(sbfs_handle *h)
         if (per_sm < 1) return fail(h, SBFS_EINVAL, "per-lane kernel shape does not fit in shared memory");
         ls.ctas = per_sm * sms;
     }
-    P.cta.threads = 512;
+    P.cta.threads = 1024;   // the autotuner's pick with Cerny members in the batch
     P.cta.ctas = sms * 4;
     P.hbm.threads = 512;
     P.hbm.ctas = sms * 4;

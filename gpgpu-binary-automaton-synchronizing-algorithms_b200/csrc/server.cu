@@ -4,24 +4,23 @@
 // One loop thread owns the GPU work; submit/poll/cancel only touch queues
 // under a mutex.  Each turn of the loop:
 //   * takes newly submitted requests;
-//   * small requests (n <= 16): whenever one of kSmallSlots mini-batch slots is
+//   * requests with n <= 20: whenever one of kSmallSlots mini-batch slots is
 //     free, packs up to max_batch of them into pinned 64-byte records, copies
 //     them in and runs the batch kernels (per-lane / warp-pooled) on the
 //     slot's own stream.  The kernels store each automaton's length and word
 //     straight into mapped host memory and then flag it, so every request is
 //     delivered as soon as its own search ends -- a mini-batch holding a
-//     2^16-subset Cerny search does not hold back the other requests in it;
-//   * large requests (n >= 17): when the previous level launch batch is done,
+//     Cerny search (C_20: 361 levels, ~1 ms in one CTA) does not hold back the
+//     other requests in it;
+//   * large requests (n >= 21): when the previous level launch batch is done,
 //     collects finished slots, admits waiting requests in arrival order while
 //     their bitmap + queue fit the arena (the 2^n-bit budget), and launches
 //     the next few levels of every admitted request (k_level.cu).  Requests
 //     that arrive while others are running are admitted at the next turn and
 //     advance together with them: their work overlaps on the device.
-//     n = 17..20 and n >= 21 run on two level engines with their own streams
-//     (the first at higher priority) and one shared arena, so an n <= 20
-//     request never waits for the wide levels of a 2^24-subset search; the
-//     big engine leaves a reserve of the arena to the first while it has
-//     anything admitted.
+//     (n = 17..20 went through level slots too, at a p99 of 7 ms at 32K
+//     requests/s: every level of a Cerny C_20 cost one launch shared with all
+//     admitted requests.  In the mini-batches a CTA runs it alone.)
 // Completion order follows the GPU, not submission order.
 #include <atomic>
 #include <chrono>
@@ -47,10 +46,9 @@ struct Request {
     double submit_ms;
 };
 
-constexpr int kSmallMaxN = 16;
-constexpr int kMidMaxN = 20;
+constexpr int kSmallMaxN = 20;
 constexpr int kWords = 12;
-constexpr int kSmallSlots = 4;   // mini-batches in flight (lanes 0..3; then n <= 20 and n >= 21 slots)
+constexpr int kSmallSlots = 4;   // mini-batches in flight (lanes 0..3; lane 4 runs the level slots)
 
 // One mini-batch of small requests in flight.
 struct SmallSlot {
@@ -87,11 +85,11 @@ struct sbfs_server {
     // stats (mutex-protected)
     sbfs_server_stats st{};
     // loop-owned
-    std::deque<Request> pend_small, pend_mid, pend_big;
+    std::deque<Request> pend_small, pend_big;
     SmallSlot small[kSmallSlots];
     unsigned int next_tag = 1;
-    Arena arena;                                   // shared by both level engines
-    LevelEngine mid, big;                          // n = 17..20 / n >= 21
+    Arena arena;                                   // HBM budget of the admitted large requests
+    LevelEngine big;                               // level slots for n >= 21
     std::unordered_map<long long, Request> large;   // admitted, keyed by id
     std::string error;
 
@@ -214,7 +212,7 @@ void run_loop(sbfs_server *s)
             std::unique_lock<std::mutex> lock(s->mu);
             bool small_busy = false;
             for (const SmallSlot &S : s->small) small_busy |= S.busy;
-            if (s->incoming.empty() && s->pend_small.empty() && s->pend_mid.empty() && s->pend_big.empty() &&
+            if (s->incoming.empty() && s->pend_small.empty() && s->pend_big.empty() &&
                 !small_busy && s->large.empty()) {
                 if (s->stopping) break;
                 s->cv_in.wait_for(lock, std::chrono::milliseconds(2));
@@ -228,7 +226,7 @@ void run_loop(sbfs_server *s)
                     lock.lock();
                     continue;
                 }
-                (r.n <= kSmallMaxN ? s->pend_small : r.n <= kMidMaxN ? s->pend_mid : s->pend_big).push_back(r);
+                (r.n <= kSmallMaxN ? s->pend_small : s->pend_big).push_back(r);
                 progress = true;
             }
         }
@@ -237,39 +235,31 @@ void run_loop(sbfs_server *s)
             if (S.busy) progress |= poll_small(s, S);
         for (SmallSlot &S : s->small)
             if (!S.busy && !s->pend_small.empty()) progress |= launch_small(s, S);
-        // large paths
-        const size_t mid_reserve =
-            std::min(s->arena.capacity() / 4, 32 * LevelEngine::footprint(kMidMaxN));
-        for (int e = 0; e < 2; ++e) {
-            LevelEngine &E = e == 0 ? s->mid : s->big;
-            std::deque<Request> &pend = e == 0 ? s->pend_mid : s->pend_big;
-            if (E.launched() && E.ready()) {
-                fin.clear();
-                E.collect(fin);
-                for (auto &f : fin) {
-                    auto it = s->large.find(f.tag);
-                    if (it == s->large.end()) continue;
-                    complete(s, it->second, f.state == kSlotDone ? SBFS_OK : SBFS_ECUDA, f.len, f.word);
-                    s->large.erase(it);
-                }
-                progress = true;
+        // large path
+        LevelEngine &E = s->big;
+        if (E.launched() && E.ready()) {
+            fin.clear();
+            E.collect(fin);
+            for (auto &f : fin) {
+                auto it = s->large.find(f.tag);
+                if (it == s->large.end()) continue;
+                complete(s, it->second, f.state == kSlotDone ? SBFS_OK : SBFS_ECUDA, f.len, f.word);
+                s->large.erase(it);
             }
-            if (!E.launched()) {
-                while (!pend.empty()) {
-                    const Request &r = pend.front();
-                    if (e == 1 && E.in_flight() > 0 &&
-                        s->arena.used() + LevelEngine::footprint(r.n) + mid_reserve > s->arena.capacity())
-                        break;
-                    if (E.admit(nullptr, 32, r.n, (long long)r.id, r.a, r.b) < 0) break;
-                    s->large.emplace((long long)r.id, r);
-                    pend.pop_front();
-                }
-                if (E.in_flight() > 0) {
-                    E.launch(s->cfg.max_levels, none, 4 * s->cfg.max_levels);
-                    std::lock_guard<std::mutex> lock(s->mu);
-                    s->st.level_launches += s->cfg.max_levels;
-                    progress = true;
-                }
+            progress = true;
+        }
+        if (!E.launched()) {
+            while (!s->pend_big.empty()) {
+                const Request &r = s->pend_big.front();
+                if (E.admit(nullptr, 32, r.n, (long long)r.id, r.a, r.b) < 0) break;
+                s->large.emplace((long long)r.id, r);
+                s->pend_big.pop_front();
+            }
+            if (E.in_flight() > 0) {
+                E.launch(s->cfg.max_levels, none, 4 * s->cfg.max_levels);
+                std::lock_guard<std::mutex> lock(s->mu);
+                s->st.level_launches += s->cfg.max_levels;
+                progress = true;
             }
         }
         {
@@ -278,8 +268,7 @@ void run_loop(sbfs_server *s)
                 s->arena.reset_peak();
                 s->reset_peak = false;
             }
-            s->st.pending = (int64_t)(s->incoming.size() + s->pend_small.size() + s->pend_mid.size() +
-                                      s->pend_big.size());
+            s->st.pending = (int64_t)(s->incoming.size() + s->pend_small.size() + s->pend_big.size());
             size_t small_left = 0;
             for (const SmallSlot &S : s->small) small_left += S.busy ? S.left : 0;
             s->st.in_flight = (int64_t)(small_left + s->large.size());
@@ -326,8 +315,8 @@ sbfs_status sbfs_server_start(const sbfs_server_config *cfg, sbfs_server **out)
     sbfs_config hc;
     sbfs_config_default(&hc);
     hc.device = s->cfg.device;
-    // small batches, n <= 20 level slots, n >= 21 level slots: stream priority in that order
-    hc.streams = kSmallSlots + 2;
+    // small batches, then the level slots: stream priority in that order
+    hc.streams = kSmallSlots + 1;
     sbfs_status st = sbfs_create(&hc, &s->h);
     if (st) {
         delete s;
@@ -347,12 +336,10 @@ sbfs_status sbfs_server_start(const sbfs_server_config *cfg, sbfs_server **out)
             break;
         std::memset(S.h_flags.ptr, 0, mb * 4);
     }
-    if (e == cudaSuccess && (e = s->arena.reserve((size_t)s->cfg.arena_bytes)) == cudaSuccess &&
-        (e = s->mid.init(s->h->sm_count, 0, s->h->lanes[kSmallSlots].stream, &s->arena)) == cudaSuccess)
-        e = s->big.init(s->h->sm_count, 0, s->h->lanes[kSmallSlots + 1].stream, &s->arena);
+    if (e == cudaSuccess && (e = s->arena.reserve((size_t)s->cfg.arena_bytes)) == cudaSuccess)
+        e = s->big.init(s->h->sm_count, 0, s->h->lanes[kSmallSlots].stream, &s->arena);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        s->mid.destroy();
         s->big.destroy();
         s->arena.release();
         for (SmallSlot &S : s->small) {
@@ -455,7 +442,6 @@ sbfs_status sbfs_server_stop(sbfs_server *s)
     cudaSetDevice(s->h->device);
     for (size_t i = 1; i < s->h->lanes.size(); ++i) cudaStreamSynchronize(s->h->lanes[i].stream);
     cudaStreamSynchronize(s->h->lanes[0].stream);
-    s->mid.destroy();
     s->big.destroy();
     s->arena.release();
     for (SmallSlot &S : s->small) {

@@ -200,14 +200,13 @@ SBFS_API int32_t sbfs_describe_plan(sbfs_handle *h, char *buf, int32_t len);
 
 /* ---------------------------------------------------------------------------
  * Serving: a request loop on its own thread.  Requests (one automaton each)
- * are admitted as they arrive: automata with n <= 16 are gathered into
+ * are admitted as they arrive: automata with n <= 20 are gathered into
  * mini-batches (several in flight) and solved by the batch kernels, which
- * deliver each result as soon as its own search ends; automata with n >= 17
+ * deliver each result as soon as its own search ends; automata with n >= 21
  * are admitted into device-resident BFS slots while their 2^n-bit bitmap and
  * queue fit the arena budget, and advance a few levels per launch alongside
- * every other admitted request of their size band (17..20 and 21..28 run
- * separately), so a request that arrives while others run is taken in as soon
- * as memory frees up.  No reference counterpart (the reference solves fixed
+ * every other admitted request, so a request that arrives while others run is
+ * taken in as soon as memory frees up.  No reference counterpart (the reference solves fixed
  * batches only, GPGPU/Program.cs:76-111).
  * ------------------------------------------------------------------------- */
 typedef struct sbfs_server sbfs_server;
