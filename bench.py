@@ -68,6 +68,7 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=1.5, help="wall time of the CPU baseline sample")
     ap.add_argument("--plain-sample", type=int, default=2000)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="n12: skip the serving-latency summary")
     ap.add_argument("--no-tune", action="store_true", help="keep the default kernel shapes")
     ap.add_argument("--no-graph", action="store_true", help="launch every step directly, no CUDA graphs")
     ap.add_argument("--chunk", type=int, default=0, help="host path: automata per chunk (0 = library default)")
@@ -403,6 +404,17 @@ def run_sbfs(args):
                          f"({kind}; C restatement, the C# reference cannot run here)"}
 
     if rank == 0:
+        # p50/p99 of the metric's serving half: single-automaton requests through the
+        # serving loop (n log-uniform 8..24, 5 % Cerny), at 32K requests/s and all at once
+        serving = None
+        if args.workload == "n12" and not args.no_serving:
+            def brief(e):
+                return {"offered_per_s": e["offered_per_s"], "achieved_per_s": e["achieved_automata_per_s"],
+                        "p50_ms_n_le_20": e["latency_ms_n_le_20"]["p50"],
+                        "p99_ms_n_le_20": e["latency_ms_n_le_20"]["p99"],
+                        "p99_ms_all": e["latency_ms"]["p99"]}
+            serving = {"requests": 10_000, "sweep": [brief(e) for e in serve_sweep(10_000, [32000.0, 0.0])],
+                       "full_sweep": "bench.py --workload serving"}
         # roofline of the dominant kernel (the step is one BFS launch plus tiny bookkeeping)
         kern = [c["kernel"] for c in plan.get("classes", []) if c["max_n"] >= wl["max_n"]][:1]
         kernel = kern[0] if kern else "k_pool"
@@ -448,6 +460,8 @@ def run_sbfs(args):
                         "max_length": int(lens.max()) if count else 0},
             "plan": plan,
         }
+        if serving:
+            line["serving"] = serving
         print(json.dumps(line), flush=True)
     eng.close()
     if dist:
@@ -460,7 +474,10 @@ def run_sbfs(args):
 # serving: open-loop Poisson arrivals of single-automaton requests
 # ---------------------------------------------------------------------------
 
-def run_serving(args):
+def serve_sweep(count, rates, max_batch=0, max_levels=0):
+    """Open-loop Poisson sweep of single-automaton requests through the serving
+    loop (n log-uniform 8..24, 5 % Cerny family); one entry per offered rate
+    (0 = all submitted at once)."""
     import threading
 
     import numpy as np
@@ -468,9 +485,6 @@ def run_serving(args):
     from sbfs import problem as P
     from sbfs.server import Server
 
-    if int(os.environ.get("RANK", "0")) != 0:
-        return 0
-    count = args.count or 20_000
     seed = 0x5EED + 3
     ns = P.log_uniform_sizes(count, 8, 24, seed)
     recs = P.uniform_maps(count, ns, seed + 1)
@@ -479,12 +493,12 @@ def run_serving(args):
         recs[i] = P.cerny_record(int(ns[i]))
     a_rows = [np.ascontiguousarray(recs[i, :ns[i]]) for i in range(count)]
     b_rows = [np.ascontiguousarray(recs[i, 32:32 + ns[i]]) for i in range(count)]
-    rates = [float(r) for r in args.rates.split(",")]
     rng = np.random.default_rng(seed)
     sweep = []
-    srv = Server(device=0, max_batch=args.max_batch, max_levels=args.max_levels)
-    # warm-up: every path once
-    warm = [srv.submit(a_rows[i], b_rows[i], int(ns[i])) for i in range(0, min(count, 2000), 7)]
+    srv = Server(device=0, max_batch=max_batch, max_levels=max_levels)
+    # warm-up: the whole request set once, so every kernel the sweep uses has been
+    # loaded and launched before anything is timed
+    warm = [srv.submit(a_rows[i], b_rows[i], int(ns[i])) for i in range(count)]
     srv.wait_all(warm)
     for rate in rates:
         srv.reset_peak()
@@ -546,6 +560,15 @@ def run_serving(args):
         sweep.append(entry)
         print(json.dumps({"serving_rate": entry}), file=sys.stderr, flush=True)
     srv.stop()
+    return sweep
+
+
+def run_serving(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    count = args.count or 20_000
+    rates = [float(r) for r in args.rates.split(",")]
+    sweep = serve_sweep(count, rates, args.max_batch, args.max_levels)
     best = max(sweep, key=lambda e: e["achieved_automata_per_s"])
     line = {
         "metric": METRIC, "value": best["achieved_automata_per_s"], "unit": UNIT, "n_gpus": 1, "steps": len(rates),
