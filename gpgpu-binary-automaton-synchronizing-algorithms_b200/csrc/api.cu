@@ -1048,8 +1048,9 @@ sbfs_status sbfs_create(const sbfs_config *cfg, sbfs_handle **out)
         return cuda_fail(nullptr, e, "creating events");
     }
     // lane i runs chunks i, i + lanes, ...: earlier lanes get higher stream
-    // priority, so an older chunk's pending CTAs (its escalation pass) are
-    // scheduled ahead of a younger chunk's and chunks complete in order
+    // priority, so an older chunk's pending CTAs (a hand-off launch after its
+    // pooled kernel) are scheduled ahead of a younger chunk's and chunks
+    // complete in order
     int prio_least = 0, prio_greatest = 0;
     if (cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest) != cudaSuccess) {
         cudaGetLastError();

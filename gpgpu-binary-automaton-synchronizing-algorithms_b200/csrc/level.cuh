@@ -100,8 +100,9 @@ public:
     int admit(const uint8_t *d_rec, int lstride, int n, long long tag, const uint8_t *host_a,
               const uint8_t *host_b);
     // upload admissions, launch `levels` level kernels -- or, when the current
-    // levels are narrow and nothing awaits set-up, one single-CTA launch that
-    // runs up to `narrow_levels` narrow levels -- then copy slot states back
+    // levels are narrow and nothing awaits set-up, one launch of an 8-CTA
+    // cluster that runs up to `narrow_levels` narrow levels -- then copy slot
+    // states back
     // (async); results go to `out` when out.out_len is set (batch mode)
     cudaError_t launch(int levels, const Batch &out, int narrow_levels = 0);
     // wait for the last launch and collect finished slots (frees their memory)

@@ -1,8 +1,9 @@
 """Serving front end: a request loop on the GPU (sbfs_server_* in include/sbfs.h).
 
-Requests are single automata.  Small ones (n <= 16) are gathered into
-mini-batches; larger ones are admitted into device-resident BFS slots as their
-2^n-bit bitmap and queue fit the memory budget, and advance level by level
+Requests are single automata.  Those with n <= 20 are gathered into
+mini-batches (several in flight) whose kernels deliver each result as soon as
+its own search ends; larger ones are admitted into device-resident BFS slots as
+their 2^n-bit bitmap and queue fit the memory budget, and advance level by level
 alongside every other admitted request (continuous batching).
 """
 from __future__ import annotations
