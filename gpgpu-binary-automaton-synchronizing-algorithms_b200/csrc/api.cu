@@ -30,6 +30,9 @@ int cta_max_ctas_per_sm(int nb_max, int threads);
 cudaError_t launch_cta(int nb_max, int threads, int ctas, const Batch &b, uint64_t *queues,
                        unsigned long long *ticket, cudaStream_t st);
 cudaError_t plan_autotune(sbfs_handle *h, Plan &plan);
+int hash_max_ctas_per_sm(int size);
+cudaError_t launch_hash(int size, int ctas, const Batch &b, int32_t *heavy_list, unsigned long long *heavy_count,
+                        unsigned long long *ticket, cudaStream_t st);
 
 cudaError_t DevBuf::reserve(size_t want)
 {
@@ -325,8 +328,25 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
             if (per_sm < 1) return fail(h, SBFS_ECUDA, "class-3 kernel does not fit on an SM");
             const int ctas = std::min(P.cta.ctas, per_sm * h->sm_count);
             CK(L.cta_queue.reserve(cta_queue_entries(nb, ctas) * sizeof(uint64_t)), "allocating CTA queues");
-            CK(launch_cta(nb, P.cta.threads, ctas, bc, L.cta_queue.as<uint64_t>(), ticket, st),
-               "launching n<=20 kernel");
+            if (plain || ticket_override || !P.class3_hash) {
+                CK(launch_cta(nb, P.cta.threads, ctas, bc, L.cta_queue.as<uint64_t>(), ticket, st),
+                   "launching n<=20 kernel");
+            } else {
+                // one warp per automaton with a hash set; searches wider than its
+                // set or longer than its level cap go to the CTA-wide kernel, same stream
+                const int hper = hash_max_ctas_per_sm(P.class3_hash);
+                if (hper < 1) return fail(h, SBFS_ECUDA, "hash-set kernel does not fit on an SM");
+                CK(L.heavy[3].reserve(escal_entries * sizeof(int32_t)), "allocating hand-off list");
+                CK(launch_hash(P.class3_hash, hper * h->sm_count, bc, L.heavy[3].as<int32_t>(),
+                               &ctr->heavy_range[3][1], ticket, st),
+                   "launching n<=20 kernel");
+                Batch bh = bc;
+                bh.order = L.heavy[3].as<int32_t>();
+                bh.range_dev = ctr->heavy_range[3];
+                CK(launch_cta(nb, P.cta.threads, ctas, bh, L.cta_queue.as<uint64_t>(), &ctr->heavy_ticket[3], st),
+                   "launching hand-off kernel");
+                *launches += 1;
+            }
         } else {
             sbfs_status ls = run_level_class(h, L, j, bc, launches);
             if (ls) return ls;
@@ -399,6 +419,7 @@ sbfs_status ensure_plan(sbfs_handle *h)
     P.hbm.ctas = sms * 4;
     P.use_pool[0] = P.use_pool[1] = h->cfg.small_kernel == 2 ? 1 : 0;
     P.class3_level = 0;
+    P.class3_hash = 1;
     P.tuned = 0;
     h->plan_ready = true;   // the tuner below runs batches with the defaults in place
     if (h->cfg.autotune) {
@@ -1101,6 +1122,10 @@ sbfs_status sbfs_destroy(sbfs_handle *h)
             if (L.ev_join[c]) cudaEventDestroy(L.ev_join[c]);
             L.spill_c[c].release();
         }
+        for (int c = 0; c < 4; ++c) {
+            L.heavy[c].release();
+            L.heavy_queue[c].release();
+        }
         if (L.level_ready) L.level.destroy();
         if (L.stream) cudaStreamDestroy(L.stream);
     }
@@ -1291,7 +1316,7 @@ int32_t sbfs_describe_plan(sbfs_handle *h, char *buf, int32_t len)
     std::snprintf(tmp, sizeof tmp,
                   "{\"class\":3,\"max_n\":20,\"kernel\":\"%s\",\"threads\":%d,\"ctas\":%d},"
                   "{\"class\":4,\"max_n\":28,\"kernel\":\"k_level\",\"threads\":512,\"slots\":%d}]}",
-                  P.class3_level ? "k_level" : "k_cta", P.cta.threads, P.cta.ctas, kMaxLevelSlots);
+                  P.class3_level ? "k_level" : P.class3_hash ? "k_hash+k_cta" : "k_cta", P.cta.threads, P.cta.ctas, kMaxLevelSlots);
     js += tmp;
     if (buf && len > 0) {
         std::strncpy(buf, js.c_str(), (size_t)len - 1);

@@ -27,10 +27,10 @@ struct DevCounters {
     // escalation list, and claims on it
     unsigned long long escal_count[2];
     unsigned long long escal_claim[2];
-    // pooled classes 0..2: automata handed to the CTA-wide kernel, as
-    // {offset 0, count} work ranges, and that kernel's tickets
-    unsigned long long heavy_range[3][2];
-    unsigned long long heavy_ticket[3];
+    // classes 0..3 (pooled warps, hash-set warps): automata handed to the
+    // CTA-wide kernel, as {offset 0, count} work ranges, and that kernel's tickets
+    unsigned long long heavy_range[4][2];
+    unsigned long long heavy_ticket[4];
     int error;
     int pad;
     unsigned long long synchronizing;             // lengths >= 0 written by this job
@@ -92,7 +92,7 @@ struct Lane {
     cudaStream_t aux[3] = {nullptr, nullptr, nullptr};
     cudaEvent_t ev_fork = nullptr, ev_join[3] = {nullptr, nullptr, nullptr};
     DevBuf spill_c[3];                         // queue spill of a pooled class, one per class
-    DevBuf heavy[3], heavy_queue[3];           // a pooled class's long searches and their CTA queues
+    DevBuf heavy[4], heavy_queue[4];           // a class's long searches and their CTA queues
     DevBuf maps, ns, len, words, spill, order, counters, ranges, cta_queue, hbm_bitmap, hbm_queue,
         escal, tickets;
     LevelEngine level;                         // device-resident slots for n > 20
@@ -120,7 +120,7 @@ struct Lane {
         uint64_t x = 1469598103934665603ull;
         for (const DevBuf *d : {&maps, &ns, &len, &words, &spill, &order, &counters, &ranges, &cta_queue, &escal,
                                 &tickets, &spill_c[0], &spill_c[1], &spill_c[2], &heavy[0], &heavy[1], &heavy[2],
-                                &heavy_queue[0], &heavy_queue[1], &heavy_queue[2]})
+                                &heavy[3], &heavy_queue[0], &heavy_queue[1], &heavy_queue[2], &heavy_queue[3]})
             x = (x ^ reinterpret_cast<uint64_t>(d->ptr)) * 1099511628211ull;
         for (const HostBuf *b : {&h_counters, &h_maps, &h_ns, &h_len, &h_words})
             x = (x ^ reinterpret_cast<uint64_t>(b->ptr)) * 1099511628211ull;
@@ -141,6 +141,9 @@ struct Plan {
     CtaShape hbm;
     int use_pool[2];     // classes 0, 1: 1 = warp-pooled kernel instead of one automaton per lane
     int class3_level;    // class 3: 1 = bitmaps in HBM (level slots) instead of shared memory (k_cta)
+    // class 3 in shared memory: hash-set warps first, k_cta for their hand-offs, with
+    // 1 = 2048 or 2 = 4096 hash slots per warp; 0 = k_cta alone
+    int class3_hash;
     int tuned;           // 1 when the autotuner (or its cache) chose the shapes
 };
 

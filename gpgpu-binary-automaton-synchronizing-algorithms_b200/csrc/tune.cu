@@ -96,7 +96,7 @@ std::string device_key(sbfs_handle *h)
     cudaDeviceProp p;
     cudaGetDeviceProperties(&p, h->device);
     char buf[320];
-    std::snprintf(buf, sizeof buf, "%s|sm%d|abi%d|v8", p.name, h->sm_count, SBFS_ABI_VERSION);
+    std::snprintf(buf, sizeof buf, "%s|sm%d|abi%d|v9", p.name, h->sm_count, SBFS_ABI_VERSION);
     for (char *c = buf; *c; ++c)
         if (*c == ' ') *c = '_';
     return buf;
@@ -106,12 +106,12 @@ std::string encode(const Plan &P)
 {
     char buf[512];
     std::snprintf(buf, sizeof buf,
-                  "c0=%d,%d,%d,%d,%d,%d,%d,%d c1=%d,%d,%d,%d,%d,%d,%d,%d c2=%d,%d,%d c3=%d,%d",
+                  "c0=%d,%d,%d,%d,%d,%d,%d,%d c1=%d,%d,%d,%d,%d,%d,%d,%d c2=%d,%d,%d c3=%d,%d,%d",
                   P.use_pool[0], P.lane[0].warps, P.lane[0].ring, P.lane[0].refill_k, P.lane[0].tail_k,
                   P.pool[0].slots, P.pool[0].warps, P.pool[0].queue_smem, P.use_pool[1], P.lane[1].warps,
                   P.lane[1].ring, P.lane[1].refill_k, P.lane[1].tail_k, P.pool[1].slots, P.pool[1].warps,
                   P.pool[1].queue_smem, P.pool[2].slots, P.pool[2].warps, P.pool[2].queue_smem, P.class3_level,
-                  P.cta.threads);
+                  P.class3_hash, P.cta.threads);
     return buf;
 }
 
@@ -119,12 +119,12 @@ bool decode(const char *s, Plan &P)
 {
     Plan Q = P;
     const int got = std::sscanf(
-        s, "c0=%d,%d,%d,%d,%d,%d,%d,%d c1=%d,%d,%d,%d,%d,%d,%d,%d c2=%d,%d,%d c3=%d,%d", &Q.use_pool[0],
+        s, "c0=%d,%d,%d,%d,%d,%d,%d,%d c1=%d,%d,%d,%d,%d,%d,%d,%d c2=%d,%d,%d c3=%d,%d,%d", &Q.use_pool[0],
         &Q.lane[0].warps, &Q.lane[0].ring, &Q.lane[0].refill_k, &Q.lane[0].tail_k, &Q.pool[0].slots,
         &Q.pool[0].warps, &Q.pool[0].queue_smem, &Q.use_pool[1], &Q.lane[1].warps, &Q.lane[1].ring,
         &Q.lane[1].refill_k, &Q.lane[1].tail_k, &Q.pool[1].slots, &Q.pool[1].warps, &Q.pool[1].queue_smem,
-        &Q.pool[2].slots, &Q.pool[2].warps, &Q.pool[2].queue_smem, &Q.class3_level, &Q.cta.threads);
-    if (got != 21) return false;
+        &Q.pool[2].slots, &Q.pool[2].warps, &Q.pool[2].queue_smem, &Q.class3_level, &Q.class3_hash, &Q.cta.threads);
+    if (got != 22) return false;
     P = Q;
     return true;
 }
@@ -276,29 +276,33 @@ cudaError_t plan_autotune(sbfs_handle *h, Plan &plan)
                 }
         P.pool[2] = best.pool[2];
     }
-    // ---- class 3: shared-memory bitmaps (per CTA) vs HBM bitmaps (level slots)
+    // ---- class 3: hash-set warps (long searches handed to k_cta) vs shared-memory
+    // bitmaps (per CTA) vs HBM bitmaps (level slots)
     // (2 % Cerny C_20 in the batch: their long thin searches set a class-3
     // launch's makespan in the mixed and serving configurations)
     if (e == cudaSuccess && (e = prepare(b, 20, 1 << 13, 50)) == cudaSuccess) {
         Plan best = P;
         double best_ms = 1e30;
-        for (int threads : {256, 512, 1024}) {
-            Plan t = P;
-            t.class3_level = 0;
-            t.cta.threads = threads;
-            h->plan = t;
-            const double ms = time_plan(b, 20, 1 << 13);
-            if (ms < best_ms) {
-                best_ms = ms;
-                best = t;
+        for (int hash : {1, 2, 0})
+            for (int threads : {256, 512, 1024}) {
+                Plan t = P;
+                t.class3_level = 0;
+                t.class3_hash = hash;
+                t.cta.threads = threads;
+                h->plan = t;
+                const double ms = time_plan(b, 20, 1 << 13);
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = t;
+                }
             }
-        }
         Plan t = P;
         t.class3_level = 1;
         h->plan = t;
         const double ms = time_plan(b, 20, 1 << 13);
         if (ms < best_ms) best = t;
         P.class3_level = best.class3_level;
+        P.class3_hash = best.class3_hash;
         P.cta = best.cta;
     }
     cudaEventDestroy(b.e0);

@@ -365,3 +365,46 @@ def test_largest_sizes(engine, oracle_mod):
     np.testing.assert_array_equal(r["len"][check], ref["len"])
     assert oracle_mod.replay(recs, r["len"], r["words"], ns=ns)[0] == 0
     assert r["first_violation"] == -1
+
+
+def _two_component_record(n, seed):
+    """States 0..h-1 and h..n-1 each closed under both letters: never synchronizing,
+    with a wide reachable power set (pairs of subsets of the two halves)."""
+    h = n // 2
+    rec = np.zeros(2 * P.RECORD_LSTRIDE, dtype=np.uint8)
+    lo = P.uniform_maps(1, h, seed)[0]
+    hi = P.uniform_maps(1, n - h, seed + 1)[0]
+    for letter in range(2):
+        base = letter * P.RECORD_LSTRIDE
+        rec[base:base + h] = lo[base:base + h]
+        rec[base + h:base + n] = hi[base:base + n - h] + h
+    return rec
+
+
+def test_n17_20_hash_set_path_and_hand_offs(engine, oracle_mod):
+    """n = 17..20: one warp per automaton with a hash set; Cerny automata (past the
+    level cap), slow permutation + merge automata and two-component automata
+    (wide, never synchronizing) go on to the CTA-wide kernel."""
+    cnt = 40_000
+    ns = P.uniform_sizes(cnt, 17, 20, 0x5EED + 17)
+    recs = P.uniform_maps(cnt, ns, 0x5EED + 17)
+    cerny = np.arange(3, cnt, 500)
+    slow = np.arange(5, cnt, 777)
+    wide = np.arange(7, cnt, 997)
+    for i in cerny:
+        recs[i] = P.cerny_record(int(ns[i]))
+    for i in slow:
+        recs[i] = P.perm_merge_record(int(ns[i]), int(i))
+    for i in wide:
+        recs[i] = _two_component_record(int(ns[i]), int(i))
+    r = engine.solve(recs, ns=ns)
+    _check(oracle_mod, recs, r, ns=ns)
+    np.testing.assert_array_equal(r["len"][cerny], (ns[cerny].astype(np.int32) - 1) ** 2)
+    assert (r["len"][wide] == -1).all()
+    # a malformed member is rejected, and the handle stays usable
+    bad = recs[:64].copy()
+    bad[40, P.RECORD_LSTRIDE + 3] = ns[40]
+    with pytest.raises(sbfs.SbfsError) as ei:
+        engine.solve(bad, ns=ns[:64])
+    assert ei.value.status == 1
+    np.testing.assert_array_equal(engine.solve(recs[:64], ns=ns[:64])["len"], r["len"][:64])
