@@ -294,6 +294,33 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
             CK(launch_lane(ls.nmax, ls.warps, ls.ring, ls.refill_k, ls.tail_k, ls.ctas, bc, list, escal_entries,
                            &ctr->escal_count[c], &ctr->escal_claim[c], ticket, LaneStream{}, cs),
                "launching per-lane kernel");
+        } else if ((c == 2 && P.class2_hash && !plain && !ticket_override) ||
+                   (c == 3 && P.class3_hash && !P.class3_level)) {
+            const int size = c == 2 ? P.class2_hash : P.class3_hash;
+            const int nb = c == 2 ? kClassMaxN[2] : std::min(20, std::max(j.ns ? j.max_n : j.n_uniform, 17));
+            const int per_sm = cta_max_ctas_per_sm(nb, P.cta.threads);
+            if (per_sm < 1) return fail(h, SBFS_ECUDA, "CTA-wide kernel does not fit on an SM");
+            const int ctas = std::min(P.cta.ctas, per_sm * h->sm_count);
+            CK(L.heavy_queue[c].reserve(cta_queue_entries(nb, ctas) * sizeof(uint64_t)), "allocating CTA queues");
+            if (plain || ticket_override) {
+                CK(launch_cta(nb, P.cta.threads, ctas, bc, L.heavy_queue[c].as<uint64_t>(), ticket, cs),
+                   "launching CTA-wide kernel");
+            } else {
+                // one warp per automaton with a hash set; searches wider than its
+                // set or longer than its level cap go to the CTA-wide kernel, same stream
+                const int hper = hash_max_ctas_per_sm(size);
+                if (hper < 1) return fail(h, SBFS_ECUDA, "hash-set kernel does not fit on an SM");
+                CK(L.heavy[c].reserve(escal_entries * sizeof(int32_t)), "allocating hand-off list");
+                CK(launch_hash(size, hper * h->sm_count, bc, L.heavy[c].as<int32_t>(), &ctr->heavy_range[c][1],
+                               ticket, cs),
+                   "launching hash-set kernel");
+                Batch bh = bc;
+                bh.order = L.heavy[c].as<int32_t>();
+                bh.range_dev = ctr->heavy_range[c];
+                CK(launch_cta(nb, P.cta.threads, ctas, bh, L.heavy_queue[c].as<uint64_t>(), &ctr->heavy_ticket[c], cs),
+                   "launching hand-off kernel");
+                *launches += 1;
+            }
         } else if (c < 3) {
             const PoolShape &s = P.pool[c];
             DevBuf &spill = fork ? L.spill_c[c] : L.spill;
@@ -328,25 +355,7 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
             if (per_sm < 1) return fail(h, SBFS_ECUDA, "class-3 kernel does not fit on an SM");
             const int ctas = std::min(P.cta.ctas, per_sm * h->sm_count);
             CK(L.cta_queue.reserve(cta_queue_entries(nb, ctas) * sizeof(uint64_t)), "allocating CTA queues");
-            if (plain || ticket_override || !P.class3_hash) {
-                CK(launch_cta(nb, P.cta.threads, ctas, bc, L.cta_queue.as<uint64_t>(), ticket, st),
-                   "launching n<=20 kernel");
-            } else {
-                // one warp per automaton with a hash set; searches wider than its
-                // set or longer than its level cap go to the CTA-wide kernel, same stream
-                const int hper = hash_max_ctas_per_sm(P.class3_hash);
-                if (hper < 1) return fail(h, SBFS_ECUDA, "hash-set kernel does not fit on an SM");
-                CK(L.heavy[3].reserve(escal_entries * sizeof(int32_t)), "allocating hand-off list");
-                CK(launch_hash(P.class3_hash, hper * h->sm_count, bc, L.heavy[3].as<int32_t>(),
-                               &ctr->heavy_range[3][1], ticket, st),
-                   "launching n<=20 kernel");
-                Batch bh = bc;
-                bh.order = L.heavy[3].as<int32_t>();
-                bh.range_dev = ctr->heavy_range[3];
-                CK(launch_cta(nb, P.cta.threads, ctas, bh, L.cta_queue.as<uint64_t>(), &ctr->heavy_ticket[3], st),
-                   "launching hand-off kernel");
-                *launches += 1;
-            }
+            CK(launch_cta(nb, P.cta.threads, ctas, bc, L.cta_queue.as<uint64_t>(), ticket, st), "launching n<=20 kernel");
         } else {
             sbfs_status ls = run_level_class(h, L, j, bc, launches);
             if (ls) return ls;
@@ -419,6 +428,7 @@ sbfs_status ensure_plan(sbfs_handle *h)
     P.hbm.ctas = sms * 4;
     P.use_pool[0] = P.use_pool[1] = h->cfg.small_kernel == 2 ? 1 : 0;
     P.class3_level = 0;
+    P.class2_hash = h->cfg.small_kernel == 2 ? 0 : 1;   // small_kernel 2: the pooled kernel up to n = 16
     P.class3_hash = 1;
     P.tuned = 0;
     h->plan_ready = true;   // the tuner below runs batches with the defaults in place
@@ -1304,6 +1314,9 @@ int32_t sbfs_describe_plan(sbfs_handle *h, char *buf, int32_t len)
                           "{\"class\":%d,\"max_n\":%d,\"kernel\":\"k_lane<%d>\",\"warps\":%d,\"ring\":%d,"
                           "\"refill\":%d,\"ctas\":%d},",
                           c, kClassMaxN[c], l.nmax, l.warps, l.ring, l.refill_k, l.ctas);
+        } else if (c == 2 && P.class2_hash) {
+            std::snprintf(tmp, sizeof tmp, "{\"class\":2,\"max_n\":16,\"kernel\":\"k_hash+k_cta\",\"slots\":%d},",
+                          P.class2_hash == 2 ? 4096 : 2048);
         } else {
             const PoolShape &q = P.pool[c];
             std::snprintf(tmp, sizeof tmp,
@@ -1316,7 +1329,8 @@ int32_t sbfs_describe_plan(sbfs_handle *h, char *buf, int32_t len)
     std::snprintf(tmp, sizeof tmp,
                   "{\"class\":3,\"max_n\":20,\"kernel\":\"%s\",\"threads\":%d,\"ctas\":%d},"
                   "{\"class\":4,\"max_n\":28,\"kernel\":\"k_level\",\"threads\":512,\"slots\":%d}]}",
-                  P.class3_level ? "k_level" : P.class3_hash ? "k_hash+k_cta" : "k_cta", P.cta.threads, P.cta.ctas, kMaxLevelSlots);
+                  P.class3_level ? "k_level" : P.class3_hash ? "k_hash+k_cta" : "k_cta", P.cta.threads, P.cta.ctas,
+                  kMaxLevelSlots);
     js += tmp;
     if (buf && len > 0) {
         std::strncpy(buf, js.c_str(), (size_t)len - 1);

@@ -16,9 +16,16 @@
 namespace sbfs {
 namespace {
 
+// One barrier per level: every thread derives the next level's bounds from the
+// entries the level appended, so the shared counters rotate and nothing a fast
+// thread writes in level L+1 is read by a slow thread finishing level L:
+//   * cnt[L % 3] counts level L's appends (positions lvl_end + count); level L
+//     zeroes cnt[(L+1) % 3], which was last read at the start of level L-1;
+//   * found[L & 1] takes level L's singleton hits; a hit ends the search, so
+//     both are reset once per automaton.
 struct CtaCtl {
-    unsigned long long found;   // min over (queue index << 1 | letter) of singleton hits
-    uint32_t lvl_start, lvl_end, tail, level;
+    unsigned long long found[2];   // min over (queue index << 1 | letter) of singleton hits
+    uint32_t cnt[3];
     int64_t k;
     int n;
     int bad;
@@ -94,17 +101,17 @@ __global__ void __launch_bounds__(1024) k_cta(Batch b, int nb_max, uint64_t *que
         if (tid == 0) {
             queue[0] = full;
             bitmap[full >> 5] |= 1u << (full & 31u);
-            ctl.found = ~0ull;
-            ctl.lvl_start = 0;
-            ctl.lvl_end = 1;
-            ctl.tail = 1;
-            ctl.level = 0;
+            ctl.found[0] = ctl.found[1] = ~0ull;
+            ctl.cnt[0] = ctl.cnt[1] = ctl.cnt[2] = 0u;
         }
         __syncthreads();
 
         int32_t len = kLenNonSync;
+        uint32_t ls = 0, le = 1, level = 0;
         while (true) {
-            const uint32_t ls = ctl.lvl_start, le = ctl.lvl_end;
+            uint32_t *cnt = &ctl.cnt[level % 3];
+            unsigned long long *found = &ctl.found[level & 1];
+            if (tid == 0) ctl.cnt[(level + 1) % 3] = 0u;
             // whole warps iterate so the push ballots stay converged
             for (uint32_t base = ls + (tid & ~31); base < le; base += blockDim.x) {
                 const uint32_t i = base + lane;
@@ -120,24 +127,24 @@ __global__ void __launch_bounds__(1024) k_cta(Batch b, int nb_max, uint64_t *que
                     const uint32_t m0 = 1u << (y0 & 31u);
                     if (!(atomicOr(&bitmap[y0 >> 5], m0) & m0)) {
                         if (is_singleton(y0))
-                            atomicMin(&ctl.found, ((unsigned long long)i << 1));
+                            atomicMin(found, ((unsigned long long)i << 1));
                         else
                             p0 = true;
                     }
                     const uint32_t m1 = 1u << (y1 & 31u);
                     if (!(atomicOr(&bitmap[y1 >> 5], m1) & m1)) {
                         if (is_singleton(y1))
-                            atomicMin(&ctl.found, ((unsigned long long)i << 1) | 1ull);
+                            atomicMin(found, ((unsigned long long)i << 1) | 1ull);
                         else
                             p1 = true;
                     }
                     ++expanded;
                 }
                 const unsigned m0 = __ballot_sync(kFull, p0), m1 = __ballot_sync(kFull, p1);
-                const int cnt = __popc(m0) + __popc(m1);
-                if (cnt) {
+                const int c = __popc(m0) + __popc(m1);
+                if (c) {
                     uint32_t pos = 0;
-                    if (lane == 0) pos = atomicAdd(&ctl.tail, (uint32_t)cnt);
+                    if (lane == 0) pos = le + atomicAdd(cnt, (uint32_t)c);
                     pos = __shfl_sync(kFull, pos, 0);
                     const unsigned lt = (1u << lane) - 1u;
                     pos += __popc(m0 & lt) + __popc(m1 & lt);
@@ -146,10 +153,8 @@ __global__ void __launch_bounds__(1024) k_cta(Batch b, int nb_max, uint64_t *que
                 }
             }
             __syncthreads();
-            const unsigned long long f = ctl.found;
-            const uint32_t tail = ctl.tail;
-            const uint32_t level = ctl.level;
-            __syncthreads();
+            const unsigned long long f = *found;
+            const uint32_t added = *cnt;
             if (f != ~0ull) {
                 len = (int32_t)level + 1;
                 if (tid == 0) {
@@ -171,7 +176,7 @@ __global__ void __launch_bounds__(1024) k_cta(Batch b, int nb_max, uint64_t *que
                 }
                 break;
             }
-            if (tail == le) {
+            if (added == 0) {
                 if (tid == 0) {
                     record_result(b, k, n, kLenNonSync);
                     if (b.out_words) {
@@ -182,12 +187,9 @@ __global__ void __launch_bounds__(1024) k_cta(Batch b, int nb_max, uint64_t *que
                 }
                 break;
             }
-            if (tid == 0) {
-                ctl.lvl_start = le;
-                ctl.lvl_end = tail;
-                ctl.level = level + 1;
-            }
-            __syncthreads();
+            ls = le;
+            le += added;
+            ++level;
         }
         __syncthreads();
     }

@@ -141,8 +141,10 @@ struct Plan {
     CtaShape hbm;
     int use_pool[2];     // classes 0, 1: 1 = warp-pooled kernel instead of one automaton per lane
     int class3_level;    // class 3: 1 = bitmaps in HBM (level slots) instead of shared memory (k_cta)
-    // class 3 in shared memory: hash-set warps first, k_cta for their hand-offs, with
-    // 1 = 2048 or 2 = 4096 hash slots per warp; 0 = k_cta alone
+    // classes 2 and 3 (class 3 in shared memory): hash-set warps first, k_cta for
+    // their hand-offs, with 1 = 2048 or 2 = 4096 hash slots per warp; 0 = the
+    // pooled kernel (class 2) or k_cta alone (class 3)
+    int class2_hash;
     int class3_hash;
     int tuned;           // 1 when the autotuner (or its cache) chose the shapes
 };

@@ -96,7 +96,7 @@ std::string device_key(sbfs_handle *h)
     cudaDeviceProp p;
     cudaGetDeviceProperties(&p, h->device);
     char buf[320];
-    std::snprintf(buf, sizeof buf, "%s|sm%d|abi%d|v9", p.name, h->sm_count, SBFS_ABI_VERSION);
+    std::snprintf(buf, sizeof buf, "%s|sm%d|abi%d|v10", p.name, h->sm_count, SBFS_ABI_VERSION);
     for (char *c = buf; *c; ++c)
         if (*c == ' ') *c = '_';
     return buf;
@@ -106,12 +106,12 @@ std::string encode(const Plan &P)
 {
     char buf[512];
     std::snprintf(buf, sizeof buf,
-                  "c0=%d,%d,%d,%d,%d,%d,%d,%d c1=%d,%d,%d,%d,%d,%d,%d,%d c2=%d,%d,%d c3=%d,%d,%d",
+                  "c0=%d,%d,%d,%d,%d,%d,%d,%d c1=%d,%d,%d,%d,%d,%d,%d,%d c2=%d,%d,%d,%d c3=%d,%d,%d",
                   P.use_pool[0], P.lane[0].warps, P.lane[0].ring, P.lane[0].refill_k, P.lane[0].tail_k,
                   P.pool[0].slots, P.pool[0].warps, P.pool[0].queue_smem, P.use_pool[1], P.lane[1].warps,
                   P.lane[1].ring, P.lane[1].refill_k, P.lane[1].tail_k, P.pool[1].slots, P.pool[1].warps,
-                  P.pool[1].queue_smem, P.pool[2].slots, P.pool[2].warps, P.pool[2].queue_smem, P.class3_level,
-                  P.class3_hash, P.cta.threads);
+                  P.pool[1].queue_smem, P.class2_hash, P.pool[2].slots, P.pool[2].warps, P.pool[2].queue_smem,
+                  P.class3_level, P.class3_hash, P.cta.threads);
     return buf;
 }
 
@@ -119,12 +119,13 @@ bool decode(const char *s, Plan &P)
 {
     Plan Q = P;
     const int got = std::sscanf(
-        s, "c0=%d,%d,%d,%d,%d,%d,%d,%d c1=%d,%d,%d,%d,%d,%d,%d,%d c2=%d,%d,%d c3=%d,%d,%d", &Q.use_pool[0],
+        s, "c0=%d,%d,%d,%d,%d,%d,%d,%d c1=%d,%d,%d,%d,%d,%d,%d,%d c2=%d,%d,%d,%d c3=%d,%d,%d", &Q.use_pool[0],
         &Q.lane[0].warps, &Q.lane[0].ring, &Q.lane[0].refill_k, &Q.lane[0].tail_k, &Q.pool[0].slots,
         &Q.pool[0].warps, &Q.pool[0].queue_smem, &Q.use_pool[1], &Q.lane[1].warps, &Q.lane[1].ring,
         &Q.lane[1].refill_k, &Q.lane[1].tail_k, &Q.pool[1].slots, &Q.pool[1].warps, &Q.pool[1].queue_smem,
-        &Q.pool[2].slots, &Q.pool[2].warps, &Q.pool[2].queue_smem, &Q.class3_level, &Q.class3_hash, &Q.cta.threads);
-    if (got != 22) return false;
+        &Q.class2_hash, &Q.pool[2].slots, &Q.pool[2].warps, &Q.pool[2].queue_smem, &Q.class3_level, &Q.class3_hash,
+        &Q.cta.threads);
+    if (got != 23) return false;
     P = Q;
     return true;
 }
@@ -251,14 +252,26 @@ cudaError_t plan_autotune(sbfs_handle *h, Plan &plan)
         P.lane[c] = best.lane[c];
         P.pool[c] = best.pool[c];
     }
-    // ---- class 2: pooled shapes ---------------------------------------------
+    // ---- class 2: hash-set warps (long searches handed to k_cta) vs pooled shapes
     if (e == cudaSuccess && (e = prepare(b, 16, 1 << 16)) == cudaSuccess) {
         Plan best = P;
         double best_ms = 1e30;
+        for (int hash : {1, 2}) {
+            if (h->cfg.small_kernel == 2) break;   // the caller asked for the pooled kernel
+            Plan t = P;
+            t.class2_hash = hash;
+            h->plan = t;
+            const double ms = time_plan(b, 16, 1 << 16);
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = t;
+            }
+        }
         for (int S : {2, 4, 8})
             for (int W : {1, 2})
                 for (int Q : {128, 256, 512}) {
                     Plan t = P;
+                    t.class2_hash = 0;
                     t.pool[2].slots = S;
                     t.pool[2].warps = W;
                     t.pool[2].queue_smem = Q;
@@ -274,6 +287,7 @@ cudaError_t plan_autotune(sbfs_handle *h, Plan &plan)
                         best = t;
                     }
                 }
+        P.class2_hash = best.class2_hash;
         P.pool[2] = best.pool[2];
     }
     // ---- class 3: hash-set warps (long searches handed to k_cta) vs shared-memory

@@ -86,7 +86,8 @@ typedef struct sbfs_config {
                                   and its results stream out in 2^17-automaton pieces; other
                                   batches in chunks of 2^18 over the streams.  > 0 = chunks of
                                   this many automata over the streams, never streamed      */
-    int32_t small_kernel;      /* n <= 12: 0 = auto (per lane), 1 = one automaton per lane, 2 = warp-pooled */
+    int32_t small_kernel;      /* n <= 16: 0 = auto (per lane up to n = 12, hash-set warps for 13..16),
+                                  1 = one automaton per lane (n <= 12), 2 = warp-pooled (n <= 16) */
     int32_t lane_ring;         /* per-lane kernel: on-chip frontier entries (power of 2); 0 = auto */
     int32_t lane_refill;       /* per-lane kernel: idle lanes that trigger a refill; 0 = auto */
     int32_t lane_warps;        /* per-lane kernel: warps per CTA; 0 = auto              */

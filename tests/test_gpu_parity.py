@@ -408,3 +408,19 @@ def test_n17_20_hash_set_path_and_hand_offs(engine, oracle_mod):
         engine.solve(bad, ns=ns[:64])
     assert ei.value.status == 1
     np.testing.assert_array_equal(engine.solve(recs[:64], ns=ns[:64])["len"], r["len"][:64])
+
+
+def test_n13_16_hash_set_and_pooled_paths(engine, oracle_mod):
+    """n = 13..16 on the hash-set warps (default) and on the warp-pooled kernel
+    (small_kernel=2), Cerny members handed to the CTA-wide kernel on both."""
+    cnt = 30_000
+    ns = P.uniform_sizes(cnt, 13, 16, 0x5EED + 13)
+    recs = P.uniform_maps(cnt, ns, 0x5EED + 13)
+    cerny = np.arange(11, cnt, 300)
+    for i in cerny:
+        recs[i] = P.cerny_record(int(ns[i]))
+    ref = oracle_mod.solve(recs, ns=ns, words=False, threads=8)
+    _check(oracle_mod, recs, engine.solve(recs, ns=ns), ns=ns, ref=ref)
+    with sbfs.Engine(device=0, small_kernel=2) as pooled:
+        _check(oracle_mod, recs, pooled.solve(recs, ns=ns), ns=ns, ref=ref)
+    assert (ref["len"][cerny] == (ns[cerny].astype(np.int32) - 1) ** 2).all()
