@@ -191,6 +191,48 @@ bool poll_small(sbfs_server *s, SmallSlot &S)
     return progress;
 }
 
+// Runs one batch of max_batch automata spanning size classes 0..3 (n = 5, 10,
+// 15, 20; seeded maps) through every mini-batch lane and waits for it.  The
+// lanes' grow-only work buffers (bucketing arrays, hand-off lists, the CTA-wide
+// kernel's queues for n = 20) reach their final size and every kernel is loaded
+// before the first request, so the loop never allocates device memory: a
+// cudaFree there would wait for the whole device.
+cudaError_t prime_small(sbfs_server *s)
+{
+    const int64_t cnt = s->cfg.max_batch;
+    const int sizes[4] = {5, 10, 15, 20};
+    for (SmallSlot &S : s->small) {
+        Lane &L = s->h->lanes[(size_t)S.lane];
+        uint8_t *rec = S.h_recs.as<uint8_t>();
+        uint8_t *ns = S.h_ns.as<uint8_t>();
+        uint64_t x = 0x9E3779B97F4A7C15ull;
+        for (int64_t i = 0; i < cnt; ++i) {
+            const int n = sizes[i & 3];
+            std::memset(rec + i * 64, 0, 64);
+            for (int j = 0; j < n; ++j)
+                for (int l = 0; l < 2; ++l) {
+                    x += 0x9E3779B97F4A7C15ull;   // splitmix64
+                    uint64_t z = x;
+                    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+                    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+                    rec[i * 64 + 32 * l + j] = (uint8_t)((z ^ (z >> 31)) % (uint64_t)n);
+                }
+            ns[i] = (uint8_t)n;
+        }
+        cudaStream_t st = L.stream;
+        cudaError_t e = cudaMemcpyAsync(S.d_recs.ptr, rec, (size_t)cnt * 64, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(S.d_ns.ptr, ns, (size_t)cnt, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return e;
+        int launches = 0;
+        if (engine_enqueue(s->h, L, S.d_recs.as<uint8_t>(), 32, S.d_ns.as<uint8_t>(), 0, 20, cnt, S.dl, S.dw, kWords,
+                           &launches, S.df, ~0u) != SBFS_OK)
+            return cudaErrorUnknown;
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+        std::memset(S.h_flags.ptr, 0, (size_t)cnt * 4);
+    }
+    return cudaSuccess;
+}
+
 bool event_done(cudaEvent_t ev)
 {
     const cudaError_t e = cudaEventQuery(ev);
@@ -338,6 +380,7 @@ sbfs_status sbfs_server_start(const sbfs_server_config *cfg, sbfs_server **out)
     }
     if (e == cudaSuccess && (e = s->arena.reserve((size_t)s->cfg.arena_bytes)) == cudaSuccess)
         e = s->big.init(s->h->sm_count, 0, s->h->lanes[kSmallSlots].stream, &s->arena);
+    if (e == cudaSuccess) e = prime_small(s);
     if (e != cudaSuccess) {
         cudaGetLastError();
         s->big.destroy();
