@@ -48,6 +48,10 @@ for _p in (PKG, os.path.join(ROOT, "oracle")):
 METRIC = "exact automata/s (n=12 batch) and p50/p99 latency, batched vs plain on 1 B200"
 UNIT = "automata/s"
 SMEM_BYTES_PER_EXPANSION = 28     # 4 pop + 2 x (4 + 4) bitmap word RMW + 2 x 4 push
+# level slots (n >= 21): bitmaps and queues live in HBM, so the search itself is
+# HBM traffic: 8 pop + 2 x (4 + 4) bitmap word RMW + 8 push (one new subset per
+# expanded subset, on average over a whole search)
+LEVEL_BYTES_PER_EXPANSION = 32
 FLUSH_BYTES = 256 << 20           # > 126 MB L2
 
 
@@ -420,6 +424,8 @@ def run_sbfs(args):
         kernel = kern[0] if kern else "k_pool"
         rec_bytes = 2 * lstride + (1 if wl["ns"] is not None else 0)
         alg_bytes = count * (rec_bytes + 4 + 8 * ws)
+        if kernel == "k_level":
+            alg_bytes += expanded_per_step * LEVEL_BYTES_PER_EXPANSION
         peaks = {}
         try:
             peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -445,6 +451,9 @@ def run_sbfs(args):
                          "frac": achieved / hbm_peak, "traffic": traffic,
                          "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                          "algorithmic_bytes_per_launch": alg_bytes,
+                         "algorithmic_bytes": ("records + results" if kernel != "k_level" else
+                                               f"records + results + {LEVEL_BYTES_PER_EXPANSION} B per expansion "
+                                               "(HBM bitmaps and queues)"),
                          "onchip": {"bound": "smem", "achieved": onchip, "peak": smem_peak, "unit": "GB/s",
                                     "frac": onchip / smem_peak,
                                     "bytes_per_expansion": SMEM_BYTES_PER_EXPANSION,

@@ -31,6 +31,8 @@ cudaError_t launch_cta(int nb_max, int threads, int ctas, const Batch &b, uint64
                        unsigned long long *ticket, cudaStream_t st);
 cudaError_t plan_autotune(sbfs_handle *h, Plan &plan);
 int hash_max_ctas_per_sm(int size);
+cudaError_t launch_sort_handoff(const Batch &b, const int32_t *list, const unsigned long long *count, int32_t *out,
+                                cudaStream_t st);
 cudaError_t launch_hash(int size, int ctas, const Batch &b, int32_t *heavy_list, unsigned long long *heavy_count,
                         unsigned long long *ticket, cudaStream_t st);
 
@@ -206,6 +208,7 @@ sbfs_status run_level_class(sbfs_handle *h, Lane &L, const Job &j, const Batch &
         CK(L.level.init(h->sm_count, level_arena_bytes(h, max_n), L.stream), "setting up level slots");
     }
     LevelEngine &E = L.level;
+    const unsigned long long expanded0 = E.expanded();
     size_t next = 0;
     int levels = 4;
     std::vector<LevelEngine::Finished> done;
@@ -229,6 +232,7 @@ sbfs_status run_level_class(sbfs_handle *h, Lane &L, const Job &j, const Batch &
         // long-running automata: fewer host round trips
         levels = done.empty() ? std::min(levels * 2, 256) : 4;
     }
+    L.level_expanded += E.expanded() - expanded0;
     return SBFS_OK;
 }
 
@@ -310,12 +314,19 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
                 // set or longer than its level cap go to the CTA-wide kernel, same stream
                 const int hper = hash_max_ctas_per_sm(size);
                 if (hper < 1) return fail(h, SBFS_ECUDA, "hash-set kernel does not fit on an SM");
-                CK(L.heavy[c].reserve(escal_entries * sizeof(int32_t)), "allocating hand-off list");
-                CK(launch_hash(size, hper * h->sm_count, bc, L.heavy[c].as<int32_t>(), &ctr->heavy_range[c][1],
-                               ticket, cs),
+                // hand-off list | the same sorted by n, largest first (mixed sizes)
+                CK(L.heavy[c].reserve(2 * escal_entries * sizeof(int32_t)), "allocating hand-off list");
+                int32_t *list = L.heavy[c].as<int32_t>();
+                CK(launch_hash(size, hper * h->sm_count, bc, list, &ctr->heavy_range[c][1], ticket, cs),
                    "launching hash-set kernel");
                 Batch bh = bc;
-                bh.order = L.heavy[c].as<int32_t>();
+                bh.order = list;
+                if (j.ns) {
+                    CK(launch_sort_handoff(bc, list, &ctr->heavy_range[c][1], list + escal_entries, cs),
+                       "launching hand-off sort");
+                    bh.order = list + escal_entries;
+                    *launches += 1;
+                }
                 bh.range_dev = ctr->heavy_range[c];
                 CK(launch_cta(nb, P.cta.threads, ctas, bh, L.heavy_queue[c].as<uint64_t>(), &ctr->heavy_ticket[c], cs),
                    "launching hand-off kernel");
@@ -464,6 +475,7 @@ sbfs_status reset_counters(sbfs_handle *h, Lane &L)
 {
     CK(L.counters.reserve(sizeof(DevCounters)), "allocating counters");
     CK(cudaMemsetAsync(L.counters.ptr, 0, sizeof(DevCounters), L.stream), "resetting counters");
+    L.level_expanded = 0;
     CK(cudaMemsetAsync(&L.counters.as<DevCounters>()->first_violation, 0xFF, sizeof(unsigned long long),
                        L.stream),
        "resetting counters");
@@ -486,7 +498,7 @@ sbfs_status finish_lane(sbfs_handle *h, Lane &L, Totals &t)
     CK(cudaEventSynchronize(L.ev_done), "waiting for a chunk");
     const DevCounters *c = L.h_counters.as<DevCounters>();
     t.error |= c->error;
-    t.expanded += (int64_t)c->expanded;
+    t.expanded += (int64_t)(c->expanded + L.level_expanded);
     t.escalated += (int64_t)(c->escal_count[0] + c->escal_count[1]);
     t.synchronizing += (int64_t)c->synchronizing;
     if (c->first_violation != ULLONG_MAX) {
@@ -663,6 +675,7 @@ sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstr
     // the kernel, behind chunk 0
     CK(cudaStreamWaitEvent(L.stream, S.ev_in0, 0), "ordering streams");
     CK(cudaMemsetAsync(L.counters.ptr, 0, sizeof(DevCounters), L.stream), "resetting counters");
+    L.level_expanded = 0;
     CK(cudaMemsetAsync(&L.counters.as<DevCounters>()->first_violation, 0xFF, sizeof(unsigned long long), L.stream),
        "resetting counters");
     CK(cudaMemsetAsync(L.escal.ptr, 0xFF, (size_t)cnt * sizeof(int32_t), L.stream), "resetting escalation list");
@@ -774,7 +787,7 @@ sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstr
         if (out_len) std::memcpy(out_len, dst_len, cnt * sizeof(int32_t));
         if (out_words) std::memcpy(out_words, dst_words, (size_t)cnt * ws * sizeof(uint64_t));
     }
-    o.expanded += (int64_t)hc->expanded;
+    o.expanded += (int64_t)(hc->expanded + L.level_expanded);
     o.escalated += esc;
     o.synchronizing += (int64_t)hc->synchronizing;
     o.error |= hc->error;
@@ -1280,7 +1293,7 @@ sbfs_status sbfs_device_wait(sbfs_handle *h, sbfs_stats *stats)
     if (stats) {
         std::memset(stats, 0, sizeof(*stats));
         stats->automata = h->device_count;
-        stats->expanded = (int64_t)c->expanded;
+        stats->expanded = (int64_t)(c->expanded + h->lanes[0].level_expanded);
         stats->escalated = (int64_t)(c->escal_count[0] + c->escal_count[1]);
         stats->synchronizing = (int64_t)c->synchronizing;
         stats->launches = h->device_launches;

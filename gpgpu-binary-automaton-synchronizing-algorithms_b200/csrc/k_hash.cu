@@ -230,6 +230,38 @@ __global__ void __launch_bounds__(HashGeom<CAP_BITS>::kWarps * 32)
     if (lane == 0 && b.expanded && expanded) atomicAdd(b.expanded, expanded);
 }
 
+// Counting sort of a hand-off list by n, largest first (one CTA): the
+// persistent CTA-wide kernel then takes the longest searches first, and the
+// short ones fill the SMs that free up (longest-processing-time order).
+__global__ void __launch_bounds__(1024) k_sort_handoff(Batch b, const int32_t *list,
+                                                       const unsigned long long *count, int32_t *out)
+{
+    __shared__ unsigned int hist[SBFS_MAX_N + 2];
+    const int tid = threadIdx.x;
+    const int64_t cnt = (int64_t)*count;
+    for (int i = tid; i < SBFS_MAX_N + 2; i += blockDim.x) hist[i] = 0u;
+    __syncthreads();
+    for (int64_t i = tid; i < cnt; i += blockDim.x) {
+        const int n = min(max(automaton_n(b, list[i]), 0), SBFS_MAX_N + 1);
+        atomicAdd(&hist[n], 1u);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        unsigned int off = 0;
+        for (int n = SBFS_MAX_N + 1; n >= 0; --n) {
+            const unsigned int c = hist[n];
+            hist[n] = off;
+            off += c;
+        }
+    }
+    __syncthreads();
+    for (int64_t i = tid; i < cnt; i += blockDim.x) {
+        const int32_t k = list[i];
+        const int n = min(max(automaton_n(b, k), 0), SBFS_MAX_N + 1);
+        out[atomicAdd(&hist[n], 1u)] = k;
+    }
+}
+
 template <int CAP_BITS>
 struct HashLaunch {
     static size_t smem() { return (size_t)HashGeom<CAP_BITS>::kWarps * sizeof(HashWarp<CAP_BITS>); }
@@ -267,6 +299,13 @@ struct HashLaunch {
 int hash_max_ctas_per_sm(int size)
 {
     return size == 2 ? HashLaunch<12>::per_sm() : size == 1 ? HashLaunch<11>::per_sm() : 0;
+}
+
+cudaError_t launch_sort_handoff(const Batch &b, const int32_t *list, const unsigned long long *count, int32_t *out,
+                                cudaStream_t st)
+{
+    k_sort_handoff<<<1, 1024, 0, st>>>(b, list, count, out);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_hash(int size, int ctas, const Batch &b, int32_t *heavy_list, unsigned long long *heavy_count,

@@ -97,6 +97,7 @@ struct Lane {
         escal, tickets;
     LevelEngine level;                         // device-resident slots for n > 20
     bool level_ready = false;
+    unsigned long long level_expanded = 0;     // subsets the level slots expanded for the current job
     HostBuf h_counters;                        // pinned copy of DevCounters
     HostBuf h_maps, h_ns, h_len, h_words;      // pinned staging for pageable callers
     // chunk bookkeeping
