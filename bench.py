@@ -48,10 +48,10 @@ for _p in (PKG, os.path.join(ROOT, "oracle")):
 METRIC = "exact automata/s (n=12 batch) and p50/p99 latency, batched vs plain on 1 B200"
 UNIT = "automata/s"
 SMEM_BYTES_PER_EXPANSION = 28     # 4 pop + 2 x (4 + 4) bitmap word RMW + 2 x 4 push
-# level slots (n >= 21): bitmaps and queues live in HBM, so the search itself is
-# HBM traffic: 8 pop + 2 x (4 + 4) bitmap word RMW + 8 push (one new subset per
-# expanded subset, on average over a whole search)
-LEVEL_BYTES_PER_EXPANSION = 32
+# level slots (n >= 21): bitmaps and frontiers live in HBM, so the search itself
+# is HBM traffic: 4 E frontier reads + 8 E bitmap-word probes + 4 D bitmap writes
+# + 4 D frontier writes, with D (discoveries) = E (expansions) over a whole search
+LEVEL_BYTES_PER_EXPANSION = 20
 FLUSH_BYTES = 256 << 20           # > 126 MB L2
 
 
