@@ -99,6 +99,7 @@ constexpr int kDefaultLanes = 4;
 // CTA-wide kernel: random automata with n <= 20 stay below 40 (max 36 in 20K
 // samples at n = 20), a Cerny automaton needs (n-1)^2
 constexpr int kPoolLevelCap = 48;
+constexpr int kHandoffThreads16 = 256;   // CTA width of the CTA-wide kernel on n <= 16 hand-offs
 constexpr int64_t kDefaultChunk = 1 << 18;
 
 sbfs_status fail(sbfs_handle *h, sbfs_status st, const std::string &msg)
@@ -302,12 +303,16 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
                    (c == 3 && P.class3_hash && !P.class3_level)) {
             const int size = c == 2 ? P.class2_hash : P.class3_hash;
             const int nb = c == 2 ? kClassMaxN[2] : std::min(20, std::max(j.ns ? j.max_n : j.n_uniform, 17));
-            const int per_sm = cta_max_ctas_per_sm(nb, P.cta.threads);
+            // class 2's hand-offs (Cerny C_13..C_16: a few hundred subsets per level)
+            // run 256-thread CTAs, several per SM; class 3 keeps the tuned width
+            const int threads = c == 2 && !plain && !ticket_override ? std::min(P.cta.threads, kHandoffThreads16)
+                                                                     : P.cta.threads;
+            const int per_sm = cta_max_ctas_per_sm(nb, threads);
             if (per_sm < 1) return fail(h, SBFS_ECUDA, "CTA-wide kernel does not fit on an SM");
             const int ctas = std::min(P.cta.ctas, per_sm * h->sm_count);
             CK(L.heavy_queue[c].reserve(cta_queue_entries(nb, ctas) * sizeof(uint64_t)), "allocating CTA queues");
             if (plain || ticket_override) {
-                CK(launch_cta(nb, P.cta.threads, ctas, bc, L.heavy_queue[c].as<uint64_t>(), ticket, cs),
+                CK(launch_cta(nb, threads, ctas, bc, L.heavy_queue[c].as<uint64_t>(), ticket, cs),
                    "launching CTA-wide kernel");
             } else {
                 // one warp per automaton with a hash set; searches wider than its
@@ -328,7 +333,7 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
                     *launches += 1;
                 }
                 bh.range_dev = ctr->heavy_range[c];
-                CK(launch_cta(nb, P.cta.threads, ctas, bh, L.heavy_queue[c].as<uint64_t>(), &ctr->heavy_ticket[c], cs),
+                CK(launch_cta(nb, threads, ctas, bh, L.heavy_queue[c].as<uint64_t>(), &ctr->heavy_ticket[c], cs),
                    "launching hand-off kernel");
                 *launches += 1;
             }

@@ -11,8 +11,10 @@
 //   * a hash set of 2^CAP_BITS slots, each holding subset | generation << 20;
 //     the generation changes with every automaton, so a slot from an earlier
 //     automaton reads as empty and the set is cleared once per 4095 automata;
-//   * a level-ordered queue of subset | letter-is-b << 31 with a 16-bit parent
+//   * a level-ordered queue of 16-bit entries, set slot | letter-is-b << 15
+//     (a slot keeps its subset for the whole search), with a 16-bit parent
 //     index per entry, retained for the word (GPGPU/CPU/CPU.cs:203-205).
+// 15 KB per warp at 2048 slots: five warps per CTA, three CTAs per SM.
 // The warp expands 32 subsets of the current level per step (level-
 // synchronous, as GPGPU/CPU/SlimCPUUntweaked.cs:119-184), tests the images
 // against the set (atomicCAS insert), and appends the new ones compacted by
@@ -32,7 +34,7 @@ template <int CAP_BITS>
 struct HashGeom {
     static constexpr int kCap = 1 << CAP_BITS;                  // hash slots per warp
     static constexpr uint32_t kLimit = 3u * (1u << CAP_BITS) / 4u;   // subsets a warp keeps
-    static constexpr int kWarps = CAP_BITS <= 11 ? 4 : 2;        // warps per CTA (~72 KB)
+    static constexpr int kWarps = CAP_BITS <= 11 ? 5 : 2;        // warps per CTA (~75 KB)
 };
 
 template <int CAP_BITS>
@@ -40,7 +42,7 @@ struct __align__(16) HashWarp {
     using G = HashGeom<CAP_BITS>;
     uint64_t table[5 * 16];
     uint32_t set[G::kCap];
-    uint32_t queue[G::kLimit];
+    uint16_t queue[G::kLimit];    // set slot | letter-is-b << 15
     uint16_t parent[G::kLimit];
 };
 
@@ -50,9 +52,10 @@ __device__ __forceinline__ uint32_t hash_slot(uint32_t x)
     return (x * 0x9E3779B1u) >> (32 - CAP_BITS);
 }
 
-// Inserts subset x (generation gen); true when it was not yet in the set.
+// Inserts subset x (generation gen); returns its slot when it was not yet in
+// the set, -1 otherwise.
 template <int CAP_BITS>
-__device__ __forceinline__ bool set_insert(uint32_t *set, uint32_t x, uint32_t gen)
+__device__ __forceinline__ int set_insert(uint32_t *set, uint32_t x, uint32_t gen)
 {
     constexpr int kCap = 1 << CAP_BITS;
     const uint32_t key = x | (gen << 20);
@@ -61,13 +64,13 @@ __device__ __forceinline__ bool set_insert(uint32_t *set, uint32_t x, uint32_t g
         uint32_t v = set[p];
         while ((v >> 20) != gen) {   // a slot of an earlier automaton: empty for this one
             const uint32_t prev = atomicCAS(&set[p], v, key);
-            if (prev == v) return true;
+            if (prev == v) return (int)p;
             v = prev;   // someone else took it: look at what is there now
         }
-        if (v == key) return false;
+        if (v == key) return -1;
         p = (p + 1) & (kCap - 1);
     }
-    return false;   // unreachable: the set is never more than ~3/4 full
+    return -1;   // unreachable: the set is never more than ~3/4 full
 }
 
 template <int CAP_BITS>
@@ -137,10 +140,7 @@ __global__ void __launch_bounds__(HashGeom<CAP_BITS>::kWarps * 32)
             __syncwarp();
         }
         const uint32_t full = (1u << n) - 1u;
-        if (lane == 0) {
-            set_insert<CAP_BITS>(W.set, full, gen);
-            W.queue[0] = full;
-        }
+        if (lane == 0) W.queue[0] = (uint16_t)set_insert<CAP_BITS>(W.set, full, gen);
         __syncwarp();
         // n = 1: the visited root is the only singleton, the search generates nothing new
         uint32_t head = 0, lvl_end = n > 1 ? 1u : 0u, tail = lvl_end, level = 0;
@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(HashGeom<CAP_BITS>::kWarps * 32)
             const bool has = idx < lvl_end;
             uint32_t ya = 0, yb = 0;
             if (has) {
-                const uint32_t x = W.queue[idx] & kSubsetMask;
+                const uint32_t x = W.set[W.queue[idx] & 0x7FFFu] & kSubsetMask;
                 uint64_t t = W.table[x & 15u] | W.table[16 + ((x >> 4) & 15u)] | W.table[32 + ((x >> 8) & 15u)] |
                              W.table[48 + ((x >> 12) & 15u)] | W.table[64 + ((x >> 16) & 15u)];
                 ya = (uint32_t)(t >> 32);
@@ -169,8 +169,9 @@ __global__ void __launch_bounds__(HashGeom<CAP_BITS>::kWarps * 32)
                 len = (int32_t)level + 1;
                 break;
             }
-            const bool fa = has && set_insert<CAP_BITS>(W.set, ya, gen);
-            const bool fb = has && set_insert<CAP_BITS>(W.set, yb, gen);
+            const int sa_slot = has ? set_insert<CAP_BITS>(W.set, ya, gen) : -1;
+            const int sb_slot = has ? set_insert<CAP_BITS>(W.set, yb, gen) : -1;
+            const bool fa = sa_slot >= 0, fb = sb_slot >= 0;
             const unsigned ma = __ballot_sync(kFull, fa), mb = __ballot_sync(kFull, fb);
             const uint32_t added = (uint32_t)(__popc(ma) + __popc(mb));
             if (tail + added > kHashLimit) {
@@ -180,11 +181,11 @@ __global__ void __launch_bounds__(HashGeom<CAP_BITS>::kWarps * 32)
             const unsigned lt = (1u << lane) - 1u;
             uint32_t p = tail + (uint32_t)(__popc(ma & lt) + __popc(mb & lt));
             if (fa) {
-                W.queue[p] = ya;
+                W.queue[p] = (uint16_t)sa_slot;
                 W.parent[p++] = (uint16_t)idx;
             }
             if (fb) {
-                W.queue[p] = yb | (1u << 31);
+                W.queue[p] = (uint16_t)(sb_slot | 0x8000);
                 W.parent[p] = (uint16_t)idx;
             }
             tail += added;
@@ -214,7 +215,7 @@ __global__ void __launch_bounds__(HashGeom<CAP_BITS>::kWarps * 32)
                     if (found_letter) w0 |= 1ull << level;
                     uint32_t i = found;
                     for (int d = (int)level - 1; d >= 0; --d) {
-                        if (W.queue[i] >> 31) w0 |= 1ull << d;
+                        if (W.queue[i] >> 15) w0 |= 1ull << d;
                         i = W.parent[i];
                     }
                 }
