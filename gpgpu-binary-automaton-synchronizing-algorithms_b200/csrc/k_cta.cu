@@ -11,6 +11,8 @@
 // appends new subsets with one shared atomic per warp, and moves to the next
 // level after a barrier -- the level-synchronous structure of
 // GPGPU/GPU/SlimGPUQueue.cs:314-405 without its per-thread queue atomics.
+#include <atomic>
+
 #include "common.cuh"
 
 namespace sbfs {
@@ -211,18 +213,59 @@ size_t cta_queue_entries(int nb_max, int ctas)
     return (size_t)ctas << nb_max;
 }
 
+namespace {
+
+constexpr int kMaxDevices = 16;
+
+int current_device()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    return dev;
+}
+
+// Raises the kernel's dynamic shared-memory cap once per device to the largest
+// footprint any launch asks for (n = 20), so concurrent launches of different
+// sizes never lower it under one another.
+cudaError_t cta_allow_smem()
+{
+    static std::atomic<int> done[kMaxDevices];
+    const int dev = current_device();
+    const bool cached = dev >= 0 && dev < kMaxDevices;
+    if (cached && done[dev].load(std::memory_order_acquire)) return cudaSuccess;
+    const cudaError_t e = cudaFuncSetAttribute(k_cta, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)cta_smem_bytes(20));
+    if (e == cudaSuccess && cached) done[dev].store(1, std::memory_order_release);
+    return e;
+}
+
+}  // namespace
+
 int cta_max_ctas_per_sm(int nb_max, int threads)
 {
-    const size_t smem = cta_smem_bytes(nb_max);
-    if (cudaFuncSetAttribute(k_cta, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+    // resident CTAs per (device, n, width), measured once: enqueue paths ask on every launch
+    static std::atomic<int> known[kMaxDevices][21][33];
+    if (nb_max < 1 || nb_max > 20 || threads < 32 || threads > 1024 || (threads & 31)) return 0;
+    const int dev = current_device();
+    const bool cached = dev >= 0 && dev < kMaxDevices;
+    if (cached) {
+        const int v = known[dev][nb_max][threads >> 5].load(std::memory_order_relaxed);
+        if (v > 0) return v;
+    }
+    if (cta_allow_smem() != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
     int blocks = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_cta, threads, smem) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_cta, threads, cta_smem_bytes(nb_max)) !=
+        cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
+    if (cached && blocks > 0) known[dev][nb_max][threads >> 5].store(blocks, std::memory_order_relaxed);
     return blocks;
 }
 
@@ -232,7 +275,7 @@ cudaError_t launch_cta(int nb_max, int threads, int ctas, const Batch &b, uint64
     if (nb_max < 1 || nb_max > 20 || threads < 32 || threads > 1024 || (threads & 31) || ctas < 1)
         return cudaErrorInvalidValue;
     const size_t smem = cta_smem_bytes(nb_max);
-    cudaError_t e = cudaFuncSetAttribute(k_cta, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const cudaError_t e = cta_allow_smem();
     if (e != cudaSuccess) return e;
     k_cta<<<ctas, threads, smem, st>>>(b, nb_max, queues, ticket);
     return cudaGetLastError();

@@ -1,7 +1,8 @@
-// k_hash.cu -- power-set BFS of class-3 automata (n <= 20) with one warp per
-// automaton and an open-addressed hash set as the visited store.
+// k_hash.cu -- power-set BFS of automata with 13..20 states (size classes 2
+// and 3) with one warp per automaton and an open-addressed hash set as the
+// visited store.
 //
-// A random automaton of 17..20 states is settled after a few hundred subsets
+// A random automaton of 13..20 states is settled after a few hundred subsets
 // over ~11 levels (its shortest word is at most ~36 letters), so neither a
 // 2^n-bit bitmap (128 KiB at n = 20) nor a 1024-thread CTA (k_cta.cu) pays for
 // itself: the CTA's per-level barriers and round trips dominate.  Here each
@@ -22,6 +23,8 @@
 // slots or kHashLevelCap levels (a Cerny automaton: (n-1)^2 levels) is handed
 // to the CTA-wide kernel through a list.  Random n = 17..20: 1.7 % of the
 // automata pass 1536 subsets, 0.3 % pass 4096.
+#include <atomic>
+
 #include "common.cuh"
 
 namespace sbfs {
@@ -263,15 +266,43 @@ __global__ void __launch_bounds__(1024) k_sort_handoff(Batch b, const int32_t *l
     }
 }
 
+constexpr int kMaxDevices = 16;
+
+int current_device()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    return dev;
+}
+
+// The shared-memory cap and the resident CTAs per SM are set and measured once
+// per device: the enqueue paths ask on every launch.
 template <int CAP_BITS>
 struct HashLaunch {
     static size_t smem() { return (size_t)HashGeom<CAP_BITS>::kWarps * sizeof(HashWarp<CAP_BITS>); }
     static cudaError_t prepare()
     {
-        return cudaFuncSetAttribute(k_hash<CAP_BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem());
+        static std::atomic<int> done[kMaxDevices];
+        const int dev = current_device();
+        const bool cached = dev >= 0 && dev < kMaxDevices;
+        if (cached && done[dev].load(std::memory_order_acquire)) return cudaSuccess;
+        const cudaError_t e =
+            cudaFuncSetAttribute(k_hash<CAP_BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem());
+        if (e == cudaSuccess && cached) done[dev].store(1, std::memory_order_release);
+        return e;
     }
     static int per_sm()
     {
+        static std::atomic<int> known[kMaxDevices];
+        const int dev = current_device();
+        const bool cached = dev >= 0 && dev < kMaxDevices;
+        if (cached) {
+            const int v = known[dev].load(std::memory_order_relaxed);
+            if (v > 0) return v;
+        }
         if (prepare() != cudaSuccess) {
             cudaGetLastError();
             return 0;
@@ -282,6 +313,7 @@ struct HashLaunch {
             cudaGetLastError();
             return 0;
         }
+        if (cached && blocks > 0) known[dev].store(blocks, std::memory_order_relaxed);
         return blocks;
     }
     static cudaError_t launch(int ctas, const Batch &b, int32_t *list, unsigned long long *count,
