@@ -32,7 +32,7 @@ cudaError_t launch_cta(int nb_max, int threads, int ctas, const Batch &b, uint64
 cudaError_t plan_autotune(sbfs_handle *h, Plan &plan);
 int hash_max_ctas_per_sm(int size);
 cudaError_t launch_sort_handoff(const Batch &b, const int32_t *list, const unsigned long long *count, int32_t *out,
-                                cudaStream_t st);
+                                int top_n, unsigned long long *split, cudaStream_t st);
 cudaError_t launch_hash(int size, int ctas, const Batch &b, int32_t *heavy_list, unsigned long long *heavy_count,
                         unsigned long long *ticket, cudaStream_t st);
 
@@ -326,16 +326,38 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
                    "launching hash-set kernel");
                 Batch bh = bc;
                 bh.order = list;
+                bh.range_dev = ctr->heavy_range[c];
+                // class 3, mixed sizes: the hand-offs below the class's top n run in a
+                // second launch sized for n - 1, whose halved bitmap fits two CTAs per SM
+                const bool split = j.ns && c == 3 && nb >= 18;
                 if (j.ns) {
-                    CK(launch_sort_handoff(bc, list, &ctr->heavy_range[c][1], list + escal_entries, cs),
+                    CK(launch_sort_handoff(bc, list, &ctr->heavy_range[c][1], list + escal_entries, nb,
+                                           split ? ctr->heavy_split[c] : nullptr, cs),
                        "launching hand-off sort");
                     bh.order = list + escal_entries;
                     *launches += 1;
                 }
-                bh.range_dev = ctr->heavy_range[c];
-                CK(launch_cta(nb, threads, ctas, bh, L.heavy_queue[c].as<uint64_t>(), &ctr->heavy_ticket[c], cs),
-                   "launching hand-off kernel");
-                *launches += 1;
+                if (split) {
+                    const int nb2 = nb - 1;
+                    const int per_sm2 = cta_max_ctas_per_sm(nb2, threads);
+                    if (per_sm2 < 1) return fail(h, SBFS_ECUDA, "CTA-wide kernel does not fit on an SM");
+                    const int ctas2 = std::min(P.cta.ctas, per_sm2 * h->sm_count);
+                    CK(L.heavy_queue[c].reserve(std::max(cta_queue_entries(nb, ctas), cta_queue_entries(nb2, ctas2)) *
+                                                sizeof(uint64_t)),
+                       "allocating CTA queues");
+                    bh.range_dev = ctr->heavy_split[c];
+                    CK(launch_cta(nb, threads, ctas, bh, L.heavy_queue[c].as<uint64_t>(), &ctr->heavy_ticket[c], cs),
+                       "launching hand-off kernel");
+                    bh.range_dev = ctr->heavy_split[c] + 2;
+                    CK(launch_cta(nb2, threads, ctas2, bh, L.heavy_queue[c].as<uint64_t>(), &ctr->heavy_ticket2[c],
+                                  cs),
+                       "launching hand-off kernel");
+                    *launches += 2;
+                } else {
+                    CK(launch_cta(nb, threads, ctas, bh, L.heavy_queue[c].as<uint64_t>(), &ctr->heavy_ticket[c], cs),
+                       "launching hand-off kernel");
+                    *launches += 1;
+                }
             }
         } else if (c < 3) {
             const PoolShape &s = P.pool[c];

@@ -237,8 +237,12 @@ __global__ void __launch_bounds__(HashGeom<CAP_BITS>::kWarps * 32)
 // Counting sort of a hand-off list by n, largest first (one CTA): the
 // persistent CTA-wide kernel then takes the longest searches first, and the
 // short ones fill the SMs that free up (longest-processing-time order).
+// With split, the sorted list is also described as two work ranges,
+// {0, entries with n >= top_n} and {that, the rest}, so the entries below
+// top_n can run in a launch sized for top_n - 1.
 __global__ void __launch_bounds__(1024) k_sort_handoff(Batch b, const int32_t *list,
-                                                       const unsigned long long *count, int32_t *out)
+                                                       const unsigned long long *count, int32_t *out,
+                                                       int top_n, unsigned long long *split)
 {
     __shared__ unsigned int hist[SBFS_MAX_N + 2];
     const int tid = threadIdx.x;
@@ -251,11 +255,18 @@ __global__ void __launch_bounds__(1024) k_sort_handoff(Batch b, const int32_t *l
     }
     __syncthreads();
     if (tid == 0) {
-        unsigned int off = 0;
+        unsigned int off = 0, top = 0;
         for (int n = SBFS_MAX_N + 1; n >= 0; --n) {
             const unsigned int c = hist[n];
             hist[n] = off;
             off += c;
+            if (n == top_n) top = off;   // entries with n >= top_n
+        }
+        if (split) {
+            split[0] = 0ull;
+            split[1] = top;
+            split[2] = top;
+            split[3] = (unsigned long long)cnt - top;
         }
     }
     __syncthreads();
@@ -335,9 +346,9 @@ int hash_max_ctas_per_sm(int size)
 }
 
 cudaError_t launch_sort_handoff(const Batch &b, const int32_t *list, const unsigned long long *count, int32_t *out,
-                                cudaStream_t st)
+                                int top_n, unsigned long long *split, cudaStream_t st)
 {
-    k_sort_handoff<<<1, 1024, 0, st>>>(b, list, count, out);
+    k_sort_handoff<<<1, 1024, 0, st>>>(b, list, count, out, top_n, split);
     return cudaGetLastError();
 }
 

@@ -31,6 +31,10 @@ struct DevCounters {
     // CTA-wide kernel, as {offset 0, count} work ranges, and that kernel's tickets
     unsigned long long heavy_range[4][2];
     unsigned long long heavy_ticket[4];
+    // class 3's sorted hand-offs as two work ranges (n = top, n < top) and the
+    // second launch's tickets
+    unsigned long long heavy_split[4][4];
+    unsigned long long heavy_ticket2[4];
     int error;
     int pad;
     unsigned long long synchronizing;             // lengths >= 0 written by this job
