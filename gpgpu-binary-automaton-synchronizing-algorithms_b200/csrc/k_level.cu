@@ -131,7 +131,7 @@ __device__ unsigned long long level_items(LevelSlot *slots, const uint64_t *tabl
             }
         }
         __syncthreads();
-        // reserve space per slot: one global atomic per slot with pushes this round
+        // reserve space per slot: one global atomic per slot with pushes in this pass
         for (int q = tid; q < nslots; q += blockDim.x) {
             const unsigned int c = sh.slot_count[q];
             if (c) {
