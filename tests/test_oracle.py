@@ -116,3 +116,35 @@ def test_invalid_records_rejected(oracle_mod):
     rec[0, 3] = 9  # state 9 with n = 5
     with pytest.raises(ValueError):
         oracle_mod.solve(rec, n=5)
+
+
+@pytest.mark.parametrize("n", [6, 10, 14, 18])
+def test_two_closed_components_never_synchronize(oracle_mod, n):
+    """States 0..h-1 and h..n-1 each closed under both letters: no word maps a
+    state of one half into the other, so no word synchronizes, however the
+    halves behave alone.  Each half alone is a random automaton; the oracle
+    must report -1 for the union (the GPU hand-off test plants these)."""
+    h = n // 2
+    rows = []
+    for seed in range(5):
+        lo = P.uniform_maps(1, h, 300 + seed)[0]
+        hi = P.uniform_maps(1, n - h, 400 + seed)[0]
+        rec = np.zeros(64, dtype=np.uint8)
+        for letter in range(2):
+            base = 32 * letter
+            rec[base:base + h] = lo[base:base + h]
+            rec[base + h:base + n] = hi[base:base + n - h] + h
+        rows.append(rec)
+    recs = np.stack(rows)
+    assert (oracle_mod.solve(recs, n=n, words=False)["len"] == -1).all()
+
+
+def test_permutation_automata_never_synchronize(oracle_mod):
+    """Both letters permutations: every image of the full set is the full set."""
+    rng = np.random.default_rng(11)
+    recs = np.zeros((20, 64), dtype=np.uint8)
+    ns = rng.integers(2, 21, 20).astype(np.uint8)
+    for i, n in enumerate(ns):
+        recs[i, :n] = rng.permutation(int(n))
+        recs[i, 32:32 + n] = rng.permutation(int(n))
+    assert (oracle_mod.solve(recs, ns=ns, words=False)["len"] == -1).all()
