@@ -424,3 +424,17 @@ def test_n13_16_hash_set_and_pooled_paths(engine, oracle_mod):
     with sbfs.Engine(device=0, small_kernel=2) as pooled:
         _check(oracle_mod, recs, pooled.solve(recs, ns=ns), ns=ns, ref=ref)
     assert (ref["len"][cerny] == (ns[cerny].astype(np.int32) - 1) ** 2).all()
+
+
+def test_permutation_automata_on_every_class(engine, oracle_mod):
+    """Both letters permutations never synchronize: the full set maps to itself
+    under both letters.  One batch spans every size class (n = 2..24)."""
+    rng = np.random.default_rng(12)
+    ns = np.array([2, 5, 8, 9, 12, 13, 16, 17, 20, 21, 24] * 3, dtype=np.uint8)
+    recs = np.zeros((len(ns), 64), dtype=np.uint8)
+    for i, n in enumerate(ns):
+        recs[i, :n] = rng.permutation(int(n))
+        recs[i, 32:32 + n] = rng.permutation(int(n))
+    r = engine.solve(recs, ns=ns)
+    assert (r["len"] == -1).all()
+    np.testing.assert_array_equal(r["len"], oracle_mod.solve(recs, ns=ns, words=False)["len"])
