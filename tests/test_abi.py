@@ -58,3 +58,32 @@ def test_null_arguments_are_rejected_without_a_device():
     fv = ctypes.c_int64()
     st = lib.sbfs_solve_batch(None, None, 32, None, 8, 0, None, None, 0, ctypes.byref(fv), None)
     assert st == 1
+
+
+def test_server_entry_points_reject_null_handles():
+    lib = _native.load()
+    assert lib.sbfs_server_config_default(None) == 1
+    assert lib.sbfs_server_start(None, None) == 1
+    rid = ctypes.c_uint64()
+    a = (ctypes.c_uint8 * 3)(1, 2, 0)
+    assert lib.sbfs_server_submit(None, a, a, 3, ctypes.byref(rid)) == 1
+    got = ctypes.c_int32()
+    assert lib.sbfs_server_poll(None, None, 0, ctypes.byref(got), 0) == 1
+    assert lib.sbfs_server_cancel(None, 7) == 1
+    assert lib.sbfs_server_stats_get(None, None) == 1
+    assert lib.sbfs_server_reset_peak(None) == 1
+    assert lib.sbfs_server_stop(None) == 0
+
+
+def test_noalloc_entry_rejects_bad_sizes_before_touching_a_device():
+    """The allocation-free entry point serves n <= 12 only (its fixed scratch is
+    sized for that) and checks its arguments before any CUDA call."""
+    lib = _native.load()
+    fv = ctypes.c_int64()
+    maps = (ctypes.c_uint8 * 64)()
+    for n, lstride, count in [(0, 32, 1), (13, 32, 1), (20, 32, 1), (8, 4, 1), (8, 33, 1), (8, 32, -1)]:
+        assert lib.sbfs_solve_small_noalloc(maps, lstride, n, count, None, None, 0, ctypes.byref(fv), None) == 1
+    assert lib.sbfs_solve_small_noalloc(maps, 32, 8, 1, None, None, 0, None, None) == 1   # no violation slot
+    assert lib.sbfs_solve_small_noalloc(None, 32, 8, 1, None, None, 0, ctypes.byref(fv), None) == 1
+    words = (ctypes.c_uint64 * 2)()
+    assert lib.sbfs_solve_small_noalloc(maps, 32, 8, 1, None, words, 0, ctypes.byref(fv), None) == 1
