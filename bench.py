@@ -1,16 +1,16 @@
 """bench.py -- throughput of exact shortest-synchronizing-word search on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl sbfs|reference]
-                    [--workload n12|n8|mixed|large]
+                    [--workload n12|n8|n13|mixed|large|serving]
 
 Default workload (the benchmark's headline configuration): 1,000,000 uniform
 random binary automata with n = 12 states per GPU, tight 24-byte records,
-seeded synthetic inputs.  By default the n12 and n8 batches are the
+seeded synthetic inputs.  By default the n12, n8 and n13 batches are the
 reference's own: Problem.FillArrayOfProblems with .NET System.Random and the
 benchmark's seed 1234567 + count (rank r > 0 adds 7919 * r); --inputs hash
-draws them from a counter hash instead.  One step = one pass of the power-set BFS over the
-whole batch, producing every shortest length (or the non-synchronizing flag)
-and one shortest word per automaton.
+draws them from a counter hash instead.  One step = one pass of the power-set
+BFS over the whole batch, producing every shortest length (or the
+non-synchronizing flag) and one shortest word per automaton.
 
   value    automata/s over all ranks with records already resident in HBM
            (sbfs_solve_batch_device), CUDA events on the launching stream, L2
@@ -18,15 +18,21 @@ and one shortest word per automaton.
   e2e      the same metric through sbfs_solve_batch with pinned host buffers:
            host->device copy of the records and device->host copy of lengths
            and words inside every timed step.
-  roofline the BFS kernel against HBM (algorithmic I/O bytes) and, under
-           "onchip", against shared-memory bandwidth (28 B per expansion).
+  roofline the dominant BFS kernel.  On-chip workloads (n <= 20): 28 B of
+           shared-memory traffic per expansion against the SM's shared-memory
+           bandwidth; the level slots (n >= 21): 20 B of HBM search traffic
+           per expansion against measured HBM bandwidth.
   cpu_baseline  the CPU restatement of the reference's timed solver
            (SlimCPU4bits13, Verify mode) on this host's cores, rank 0, N = 1.
+  mixed, large, n13  summaries of the other configurations, each timed on the
+           device with its own CPU restatement beside it (N = 1 only).
 
 With --impl reference the same workload runs through that CPU restatement
 only, on all host threads (the reference itself is C#/.NET and cannot run
-here).  Multi-GPU: one process per GPU (torchrun); every rank solves its own
-1M-automaton shard (weak scaling, no data-path collective).
+here); its batch is generated by the restatement's own System.Random, so that
+arm never loads the CUDA library.  Multi-GPU: one process per GPU; every rank
+solves its own 1M-automaton shard (weak scaling, no data-path collective).
+`--gpus N` outside torchrun starts the N ranks itself.
 """
 from __future__ import annotations
 
@@ -34,6 +40,7 @@ import argparse
 import json
 import os
 import signal
+import socket
 import statistics
 import subprocess
 import sys
@@ -53,26 +60,33 @@ SMEM_BYTES_PER_EXPANSION = 28     # 4 pop + 2 x (4 + 4) bitmap word RMW + 2 x 4 
 # + 4 D frontier writes, with D (discoveries) = E (expansions) over a whole search
 LEVEL_BYTES_PER_EXPANSION = 20
 FLUSH_BYTES = 256 << 20           # > 126 MB L2
+L2_NOTE = "flushed by a 256 MiB device write before every timed GPU step"
+NOMINAL_SMEM_BYTES_PER_CLK = 128  # 32 banks x 4 B per SM per clock
+# the reference's published n = 13 numbers (median automata/s, batch 2^21)
+PUBLISHED_N13 = {"SlimGPUQueue (GTX 1060)": 1953926, "SlimCPU (Ryzen 7, 16 threads)": 2281843,
+                 "source": "Cerny conjecture verification algorithms.pdf p.18, Median row"}
 
 
-def parse_args():
+def parse_args(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["sbfs", "reference"], default="sbfs")
-    ap.add_argument("--workload", choices=["n12", "n8", "mixed", "large", "serving"], default="n12")
+    ap.add_argument("--workload", choices=["n12", "n8", "n13", "mixed", "large", "serving"], default="n12")
     ap.add_argument("--rates", default="2000,8000,32000,128000,0",
                     help="serving: offered request rates per second (0 = submit all at once)")
     ap.add_argument("--count", type=int, default=0, help="automata per GPU (0 = the workload's size)")
     ap.add_argument("--max-batch", type=int, default=0, help="serving: small requests per mini-batch (0 = 8192)")
     ap.add_argument("--max-levels", type=int, default=0, help="serving: levels per launch batch (0 = 16)")
     ap.add_argument("--inputs", choices=["reference", "hash"], default="reference",
-                    help="n12/n8: the reference's System.Random batch or a counter-hash batch")
+                    help="n12/n8/n13: the reference's System.Random batch or a counter-hash batch")
     ap.add_argument("--cpu-seconds", type=float, default=1.5, help="wall time of the CPU baseline sample")
     ap.add_argument("--plain-sample", type=int, default=2000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="n12: skip the serving-latency summary")
+    ap.add_argument("--no-extra", action="store_true", help="n12: skip the mixed / large / n13 summaries")
+    ap.add_argument("--extra-steps", type=int, default=5, help="timed steps of each extra summary")
     ap.add_argument("--no-tune", action="store_true", help="keep the default kernel shapes")
     ap.add_argument("--no-graph", action="store_true", help="launch every step directly, no CUDA graphs")
     ap.add_argument("--chunk", type=int, default=0, help="host path: automata per chunk (0 = library default)")
@@ -81,45 +95,54 @@ def parse_args():
     ap.add_argument("--large-kinds", default="random,cerny,perm",
                     help="large workload: which families to include (random, cerny, perm)")
     ap.add_argument("--level-arena-mb", type=int, default=0, help="HBM budget of the n > 20 level slots")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 # ---------------------------------------------------------------------------
 # workloads
 # ---------------------------------------------------------------------------
 
-def _uniform_batch(count: int, n: int, rank: int, inputs: str, hash_seed: int):
+def _reference_batch(count: int, n: int, seed: int, lstride: int, gen: str):
+    """Problem.FillArrayOfProblems(count, n, seed): from the product library's
+    generator (gen = "sbfs") or from the CPU restatement's (gen = "oracle",
+    the reference arm, which must not load the CUDA library)."""
+    if gen == "oracle":
+        import oracle
+        return oracle.fill_array_of_problems(count, n, seed, lstride, threads=os.cpu_count() or 1)
     from sbfs import dotnet_random as D
+    return D.fill_array_of_problems(count, n, seed, lstride=lstride)
+
+
+def _uniform_batch(count: int, n: int, rank: int, inputs: str, hash_seed: int, gen: str):
     from sbfs import problem as P
     if inputs == "reference":
-        seed = D.BENCHMARK_SEED + count + 7919 * rank
-        return D.fill_array_of_problems(count, n, seed, lstride=n), f"System.Random, seed {seed}"
+        seed = 1234567 + count + 7919 * rank      # GPGPU/Program.cs:94
+        return _reference_batch(count, n, seed, n, gen), f"System.Random, seed {seed}"
     return P.repack(P.uniform_maps(count, n, hash_seed + 1000 * rank), 32, n), f"counter hash 0x{hash_seed:X}"
 
 
-def make_workload(name: str, count: int, rank: int, large_n=(24, 26, 28), kinds=("random", "cerny", "perm"),
-                  inputs: str = "reference"):
+def make_workload(name: str, count: int = 0, rank: int = 0, large_n=(24, 26, 28),
+                  kinds=("random", "cerny", "perm"), inputs: str = "reference", gen: str = "sbfs"):
     import numpy as np
     from sbfs import problem as P
 
     seed_base = 0x5EED
-    if name == "n12":
-        count = count or 1_000_000
-        recs, seed = _uniform_batch(count, 12, rank, inputs, seed_base + 1)
-        return dict(recs=recs, ns=None, n=12, lstride=12, max_n=12, count=count, seed=seed,
-                    desc=f"batched uniform: {count:,} random binary automata, n=12, lengths + shortest words")
-    if name == "n8":
-        count = count or 10_000
-        recs, seed = _uniform_batch(count, 8, rank, inputs, seed_base + 0)
-        return dict(recs=recs, ns=None, n=8, lstride=8, max_n=8, count=count, seed=seed,
-                    desc=f"plain config: {count:,} random binary automata, n=8")
+    if name in ("n12", "n8", "n13"):
+        n = int(name[1:])
+        count = count or {12: 1_000_000, 8: 10_000, 13: 1 << 21}[n]
+        recs, seed = _uniform_batch(count, n, rank, inputs, seed_base + {8: 0, 12: 1, 13: 6}[n], gen)
+        desc = {12: f"batched uniform: {count:,} random binary automata, n=12, lengths + shortest words",
+                8: f"plain config: {count:,} random binary automata, n=8",
+                13: f"published-number point: {count:,} random binary automata, n=13 (Program.cs batch)"}[n]
+        return dict(name=name, recs=recs, ns=None, n=n, lstride=n, max_n=n, count=count, seed=seed, desc=desc)
     if name == "mixed":
         count = count or 200_000
         ns = P.uniform_sizes(count, 6, 20, seed_base + 2 + 1000 * rank)
         recs = P.uniform_maps(count, ns, seed_base + 2 + 1000 * rank)
         for i in range(0, count, 100):   # 1% Cerny family
             recs[i] = P.cerny_record(int(ns[i]))
-        return dict(recs=recs, ns=ns, n=0, lstride=32, max_n=20, count=count, seed="counter hash 0x5EED",
+        return dict(name=name, recs=recs, ns=ns, n=0, lstride=32, max_n=20, count=count,
+                    seed=f"counter hash 0x{seed_base + 2 + 1000 * rank:X}",
                     desc=f"batched mixed: {count:,} automata, n uniform in 6..20, 1% Cerny family")
     if name == "large":
         rows, ns = [], []
@@ -134,10 +157,22 @@ def make_workload(name: str, count: int, rank: int, large_n=(24, 26, 28), kinds=
                 rows.append(P.perm_merge_record(n, seed_base + 5 + n)); ns.append(n)
         recs = np.stack(rows)
         ns = np.array(ns, dtype=np.uint8)
-        return dict(recs=recs, ns=ns, n=0, lstride=32, max_n=max(large_n), count=len(ns),
-                    seed="counter hash 0x5EED", desc=f"large single instances: n={','.join(map(str, large_n))} x "
-                         f"({' + '.join(kinds)})")
+        return dict(name=name, recs=recs, ns=ns, n=0, lstride=32, max_n=max(large_n), count=len(ns),
+                    seed=f"counter hash 0x{seed_base:X} + 4/5 + n",
+                    desc=f"large single instances: n={','.join(map(str, large_n))} x ({' + '.join(kinds)})")
     raise ValueError(name)
+
+
+def workload_config(wl) -> dict:
+    """The `config` object of the JSON line: identical in both arms."""
+    rec_bytes = 2 * wl["lstride"] + (1 if wl["ns"] is not None else 0)
+    return {"workload": wl["desc"], "automata_per_gpu": wl["count"], "n": wl["n"] or f"mixed, <= {wl['max_n']}",
+            "seed": wl["seed"], "record_bytes": rec_bytes, "word_stride_u64": word_stride_for(wl["max_n"]),
+            "l2": L2_NOTE, "parallelism": "automata sharded by rank, no collective on the data path"}
+
+
+def word_stride_for(max_n: int) -> int:
+    return max(1, ((max(max_n, 2) - 1) ** 2 + 63) // 64)
 
 
 # ---------------------------------------------------------------------------
@@ -151,7 +186,6 @@ class ClockSampler:
 
     def __init__(self, gpu_index: int):
         self.proc = None
-        self.lines = []
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -188,59 +222,91 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
+# ranks
+# ---------------------------------------------------------------------------
+
+def self_launch(args, argv) -> int:
+    """`--gpus N` outside torchrun: start N ranks (one process per GPU) with
+    torch.distributed.run on 127.0.0.1 and pass their output through."""
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + list(argv)
+    env = dict(os.environ)
+    env.setdefault("OMP_NUM_THREADS", "1")
+    return subprocess.call(cmd, env=env)
+
+
+def max_over_ranks(dist, x: float, device=None) -> float:
+    """Max of a per-rank float over the process group (identity without one)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
 # CPU legs (oracle restatement of the reference's CPU solver)
 # ---------------------------------------------------------------------------
 
-def cpu_throughput(wl, seconds: float, threads: int):
-    """SlimCPU4bits13 restatement (n <= 16) or SlimCPUUntweaked (otherwise) over
-    passes of the workload's records until `seconds` of wall time."""
-    import numpy as np
+def cpu_pass(wl, threads: int, lengths: bool = False):
+    """One pass of the CPU restatement over the workload: SlimCPU4bits13
+    (uniform n <= 16, Verify mode) or SlimCPUUntweaked (otherwise)."""
     import oracle
+    if wl["ns"] is None and wl["n"] <= 16:
+        r = oracle.verify4(wl["recs"], n=wl["n"], lstride=wl["lstride"], write_len=lengths, threads=threads)
+        kind = "SlimCPU4bits13 (nibble table, Verify mode)"
+    else:
+        r = oracle.solve(wl["recs"], ns=wl["ns"], n=wl["n"], lstride=wl["lstride"], words=False, threads=threads)
+        kind = "SlimCPUUntweaked (lengths)"
+    return r, kind
 
-    recs, n = wl["recs"], wl["n"]
+
+def cpu_throughput(wl, seconds: float, threads: int):
+    """Passes of the CPU restatement over the workload until `seconds` of wall time."""
     t0 = time.perf_counter()
-    done, passes = 0, 0
+    passes = 0
     while True:
-        if wl["ns"] is None and n <= 16:
-            oracle.verify4(recs, n=n, lstride=wl["lstride"], threads=threads)
-        else:
-            oracle.solve(recs, ns=wl["ns"], n=n, lstride=wl["lstride"], words=False, threads=threads)
-        done += recs.shape[0]
+        _, kind = cpu_pass(wl, threads)
         passes += 1
         if time.perf_counter() - t0 >= seconds:
             break
     dt = time.perf_counter() - t0
-    kind = "SlimCPU4bits13 (nibble table, Verify mode)" if (wl["ns"] is None and n <= 16) else \
-        "SlimCPUUntweaked (lengths)"
-    return done / dt, dt, passes, kind
+    return wl["count"] * passes / dt, dt, passes, kind
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    wl = make_workload(args.workload, args.count, 0, tuple(int(x) for x in args.large_n.split(",")),
-                       tuple(args.large_kinds.split(",")), args.inputs)
-    threads = os.cpu_count() or 1
     import oracle
 
     oracle.build()
+    wl = make_workload(args.workload, args.count, 0, tuple(int(x) for x in args.large_n.split(",")),
+                       tuple(args.large_kinds.split(",")), args.inputs, gen="oracle")
+    threads = os.cpu_count() or 1
     for _ in range(max(args.warmup, 0)):
-        cpu_throughput(wl, 0.0, threads)
+        cpu_pass(wl, threads)
     step_ms = []
+    kind = ""
     for _ in range(args.steps):
-        rate, dt, passes, kind = cpu_throughput(wl, 0.0, threads)
-        step_ms.append(dt * 1e3)
+        t0 = time.perf_counter()
+        _, kind = cpu_pass(wl, threads)
+        step_ms.append((time.perf_counter() - t0) * 1e3)
     ms = statistics.mean(step_ms)
     value = wl["count"] / (ms / 1e3)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u16", "data": "synthetic", "impl": "reference",
-        "config": {"workload": wl["desc"], "automata": wl["count"], "n": wl["n"] or "6..28", "seed": wl["seed"]},
+        "config": workload_config(wl),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{args.steps} passes over the full {wl['count']:,}-automaton batch "
-                                   f"({kind}, C restatement; the C# reference cannot run here)"},
+                                   f"({kind}, C restatement; the C# reference cannot run here); batch from "
+                                   "the restatement's own System.Random"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -251,15 +317,66 @@ def run_reference(args):
 # GPU arm
 # ---------------------------------------------------------------------------
 
+def load_profile_json(name: str) -> dict:
+    """A committed ncu / microbenchmark summary under profiles/ (or {})."""
+    try:
+        return json.load(open(os.path.join(ROOT, "profiles", name)))
+    except (OSError, ValueError):
+        return {}
+
+
 def load_traffic(kernel: str):
     """DRAM bytes per launch from the committed ncu summary of this kernel, if any."""
-    path = os.path.join(ROOT, "profiles", "traffic.json")
-    try:
-        d = json.load(open(path))
-    except (OSError, ValueError):
-        return None
-    ent = d.get(kernel)
+    ent = load_profile_json("traffic.json").get(kernel)
     return ent.get("dram_bytes_per_launch") if isinstance(ent, dict) else None
+
+
+class DeviceLeg:
+    """Device-resident solve of one workload: records, lengths, words and the
+    violation word in HBM, all work on one stream."""
+
+    def __init__(self, eng, wl, dev, stream):
+        import torch
+        self.eng, self.wl, self.stream = eng, wl, stream
+        self.ws = word_stride_for(wl["max_n"])
+        self.d_maps = torch.from_numpy(wl["recs"]).to(dev)
+        self.d_ns = torch.from_numpy(wl["ns"]).to(dev) if wl["ns"] is not None else None
+        self.d_len = torch.empty(wl["count"], dtype=torch.int32, device=dev)
+        self.d_words = torch.empty((wl["count"], self.ws), dtype=torch.int64, device=dev)
+        self.d_fv = torch.empty(1, dtype=torch.int64, device=dev)
+
+    def step(self):
+        wl = self.wl
+        self.eng.solve_device(self.d_maps, wl["lstride"], wl["count"], n=wl["n"], d_ns=self.d_ns,
+                              max_n=wl["max_n"], d_len=self.d_len, d_words=self.d_words, word_stride=self.ws,
+                              d_first_violation=self.d_fv, stream=self.stream)
+
+    def timed(self, steps: int, warmup: int, flush, barrier=None, sampler_factory=None):
+        """Per-step device times (ms) with L2 flushed before every step, the
+        last step's statistics and the clock summary (when sampled)."""
+        import torch
+        for i in range(warmup):
+            flush.fill_(i)
+            self.step()
+            self.eng.wait_device()
+        sampler = sampler_factory() if sampler_factory else None
+        if barrier:
+            barrier()
+        else:
+            torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for i in range(steps):
+            flush.fill_(i + 1)                 # untimed: evicts the records from L2
+            evs[i][0].record(self.stream)
+            self.step()
+            evs[i][1].record(self.stream)
+        if barrier:
+            barrier()
+        else:
+            torch.cuda.synchronize()
+        stats = self.eng.wait_device()
+        clk = sampler.stop() if sampler else None
+        return [a.elapsed_time(b) for a, b in evs], stats, clk
 
 
 def run_sbfs(args):
@@ -284,10 +401,11 @@ def run_sbfs(args):
     else:
         torch.cuda.set_device(0)
     dev = torch.device("cuda", torch.cuda.current_device())
+    props = torch.cuda.get_device_properties(dev)
     wl = make_workload(args.workload, args.count, rank, tuple(int(x) for x in args.large_n.split(",")),
                        tuple(args.large_kinds.split(",")), args.inputs)
     count, lstride = wl["count"], wl["lstride"]
-    ws = sbfs.word_stride_for(wl["max_n"])
+    ws = word_stride_for(wl["max_n"])
     import tempfile
     tune_cache = os.path.join(tempfile.gettempdir(), "sbfs_tune_cache.txt")
     eng = sbfs.Engine(device=dev.index, autotune=not args.no_tune, tune_cache=tune_cache,
@@ -300,54 +418,24 @@ def run_sbfs(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(x: float) -> float:
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     # ---- device-resident leg ------------------------------------------------
     # a dedicated stream: the events, the L2 flush and the library's kernels all
     # go on it (the legacy default stream would hand the library a NULL stream)
     stream = torch.cuda.Stream(device=dev)
     torch.cuda.set_stream(stream)
-    d_maps = torch.from_numpy(wl["recs"]).to(dev)
-    d_ns = torch.from_numpy(wl["ns"]).to(dev) if wl["ns"] is not None else None
-    d_len = torch.empty(count, dtype=torch.int32, device=dev)
-    d_words = torch.empty((count, ws), dtype=torch.int64, device=dev)
-    d_fv = torch.empty(1, dtype=torch.int64, device=dev)
     flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
-
-    def step_device():
-        eng.solve_device(d_maps, lstride, count, n=wl["n"], d_ns=d_ns, max_n=wl["max_n"], d_len=d_len,
-                         d_words=d_words, word_stride=ws, d_first_violation=d_fv, stream=stream)
-
-    for i in range(args.warmup):
-        flush.fill_(i)
-        step_device()
-        eng.wait_device()
+    leg = DeviceLeg(eng, wl, dev, stream)
     visible = [v for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip().isdigit()]
     gpu_index = int(visible[dev.index]) if dev.index < len(visible) else dev.index
-    clocks = ClockSampler(gpu_index) if rank == 0 else None
-    barrier()
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    for i in range(args.steps):
-        flush.fill_(i + 1)                 # untimed: evicts the records from L2
-        evs[i][0].record(stream)
-        step_device()
-        evs[i][1].record(stream)
-    barrier()
-    stats = eng.wait_device()
-    clk = clocks.stop() if clocks else None
-    step_ms = [a.elapsed_time(b) for a, b in evs]
+    step_ms, stats, clk = leg.timed(args.steps, args.warmup, flush, barrier,
+                                    (lambda: ClockSampler(gpu_index)) if rank == 0 else None)
     ms = statistics.mean(step_ms)
-    ms_max = max_over_ranks(ms)
+    ms_max = max_over_ranks(dist, ms, dev)
     value = count * world / (ms_max / 1e3)
     launches_per_step = int(stats.get("launches", 0))
     expanded_per_step = int(stats.get("expanded", 0))
-    fv = int(d_fv.item())
-    lens = d_len.cpu().numpy()
+    fv = int(leg.d_fv.item())
+    lens = leg.d_len.cpu().numpy()
     sync_frac = float((lens >= 0).mean()) if count else 0.0
 
     # ---- end-to-end leg through the host API ----------------------------------
@@ -371,10 +459,10 @@ def run_sbfs(args):
                           lstride=lstride, word_stride=ws, out=out)
             e2e_ms.append((time.perf_counter() - t0) * 1e3)
         barrier()
-        e2e_mean = max_over_ranks(statistics.mean(e2e_ms))
+        e2e_mean = max_over_ranks(dist, statistics.mean(e2e_ms), dev)
         st = r["stats"]
         e2e = {"value": count * world / (e2e_mean / 1e3), "unit": UNIT,
-               "h2d_bytes_per_step": int(st["h2d_bytes"]), "d2h_bytes_per_step": int(st["d2h_bytes"]) + 0,
+               "h2d_bytes_per_step": int(st["h2d_bytes"]), "d2h_bytes_per_step": int(st["d2h_bytes"]),
                "ms_per_step": e2e_mean,
                "latency_ms": {"p50": statistics.median(e2e_ms),
                               "p99": sorted(e2e_ms)[min(len(e2e_ms) - 1, int(0.99 * len(e2e_ms)))]}}
@@ -400,65 +488,68 @@ def run_sbfs(args):
 
     # ---- CPU baseline (rank 0, N = 1) --------------------------------------
     cpu = None
+    threads = os.cpu_count() or 1
     if rank == 0 and world == 1:
-        threads = os.cpu_count() or 1
         rate, dt, passes, kind = cpu_throughput(wl, args.cpu_seconds, threads)
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{passes} passes over the same {count:,}-automaton batch in {dt:.2f} s wall "
                          f"({kind}; C restatement, the C# reference cannot run here)"}
 
+    line = None
     if rank == 0:
-        # p50/p99 of the metric's serving half: single-automaton requests through the
-        # serving loop (n log-uniform 8..24, 5 % Cerny), at 32K requests/s and all at once
-        serving = None
-        if args.workload == "n12" and not args.no_serving:
-            def brief(e):
-                return {"offered_per_s": e["offered_per_s"], "achieved_per_s": e["achieved_automata_per_s"],
-                        "p50_ms_n_le_20": e["latency_ms_n_le_20"]["p50"],
-                        "p99_ms_n_le_20": e["latency_ms_n_le_20"]["p99"],
-                        "p99_ms_all": e["latency_ms"]["p99"]}
-            serving = {"requests": 10_000, "sweep": [brief(e) for e in serve_sweep(10_000, [32000.0, 0.0])],
-                       "full_sweep": "bench.py --workload serving"}
         # roofline of the dominant kernel (the step is one BFS launch plus tiny bookkeeping)
         kern = [c["kernel"] for c in plan.get("classes", []) if c["max_n"] >= wl["max_n"]][:1]
         kernel = kern[0] if kern else "k_pool"
-        rec_bytes = 2 * lstride + (1 if wl["ns"] is not None else 0)
-        alg_bytes = count * (rec_bytes + 4 + 8 * ws)
-        if kernel == "k_level":
-            alg_bytes += expanded_per_step * LEVEL_BYTES_PER_EXPANSION
         peaks = {}
         try:
             peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         except (OSError, ValueError):
             pass
         hbm_peak = peaks.get("hbm_gbs", 6650.0)
-        achieved = alg_bytes / (ms / 1e3) / 1e9
-        sm_clock_ghz = (clk or {}).get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
-        smem_peak = 148 * 128 * (sm_clock_ghz / 1e3)   # GB/s at the measured SM clock
-        onchip = expanded_per_step * SMEM_BYTES_PER_EXPANSION / (ms / 1e3) / 1e9
-        traffic = load_traffic(kernel)
+        hbm_src = "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback 6.65 TB/s"
+        rec_bytes = 2 * lstride + (1 if wl["ns"] is not None else 0)
+        io_bytes = count * (rec_bytes + 4 + 8 * ws)
+        sm_clock_mhz = (clk or {}).get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
+        onchip_cal = load_profile_json("onchip.json")
+        smem_bpc = onchip_cal.get("smem_bytes_per_clk_per_sm")
+        smem_src = (f"measured {smem_bpc:.1f} B/clk/SM ({onchip_cal.get('source', 'profiles/onchip.json')}) x "
+                    f"{props.multi_processor_count} SMs x sampled SM clock") if smem_bpc else \
+            f"nominal {NOMINAL_SMEM_BYTES_PER_CLK} B/clk/SM x {props.multi_processor_count} SMs x sampled SM clock"
+        smem_peak = props.multi_processor_count * (smem_bpc or NOMINAL_SMEM_BYTES_PER_CLK) * sm_clock_mhz / 1e3
+        io = {"bound": "hbm", "achieved": io_bytes / (ms / 1e3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+              "frac": io_bytes / (ms / 1e3) / 1e9 / hbm_peak, "algorithmic_bytes_per_launch": io_bytes,
+              "algorithmic_bytes": "records in + lengths and words out", "peak_source": hbm_src}
+        kcal = onchip_cal.get("kernels", {}).get(kernel.split("+")[0], {})
+        if kernel == "k_level":
+            search = expanded_per_step * LEVEL_BYTES_PER_EXPANSION
+            achieved = (search + io_bytes) / (ms / 1e3) / 1e9
+            roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                        "frac": achieved / hbm_peak, "traffic": load_traffic(kernel), "peak_source": hbm_src,
+                        "algorithmic_bytes_per_launch": search + io_bytes,
+                        "algorithmic_bytes": f"records + results + {LEVEL_BYTES_PER_EXPANSION} B per expansion "
+                                             "(HBM bitmaps and queues)",
+                        "expansions_per_launch": expanded_per_step}
+        else:
+            achieved = expanded_per_step * SMEM_BYTES_PER_EXPANSION / (ms / 1e3) / 1e9
+            roofline = {"bound": "smem", "achieved": achieved, "peak": smem_peak, "unit": "GB/s",
+                        "frac": achieved / smem_peak, "traffic": load_traffic(kernel), "peak_source": smem_src,
+                        "bytes_per_expansion": SMEM_BYTES_PER_EXPANSION,
+                        "expansions_per_launch": expanded_per_step,
+                        "algorithmic_bytes": "28 B of shared-memory traffic per expansion (4 pop + 2 x (4 + 4) "
+                                             "bitmap-word read-modify-write + 2 x 4 push)",
+                        "hbm_io": io}
+        if kcal:
+            roofline["issue_slots_busy"] = kcal.get("issue_active")
+            roofline["warps_per_sm"] = kcal.get("warps_per_sm")
+            roofline["ncu_source"] = kcal.get("source")
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u16", "data": "synthetic",
-            "config": {"workload": wl["desc"], "automata_per_gpu": count, "n": wl["n"] or "mixed",
-                       "record_bytes": rec_bytes, "word_stride_u64": ws, "kernel": kernel,
-                       "l2": "flushed by a 256 MiB write before every timed step",
-                       "parallelism": f"{world} GPU(s), automata sharded by rank, no collective on the data path",
-                       "seed": wl["seed"]},
+            "config": workload_config(wl),
+            "kernel": kernel,
             "e2e": e2e,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                         "frac": achieved / hbm_peak, "traffic": traffic,
-                         "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-                         "algorithmic_bytes_per_launch": alg_bytes,
-                         "algorithmic_bytes": ("records + results" if kernel != "k_level" else
-                                               f"records + results + {LEVEL_BYTES_PER_EXPANSION} B per expansion "
-                                               "(HBM bitmaps and queues)"),
-                         "onchip": {"bound": "smem", "achieved": onchip, "peak": smem_peak, "unit": "GB/s",
-                                    "frac": onchip / smem_peak,
-                                    "bytes_per_expansion": SMEM_BYTES_PER_EXPANSION,
-                                    "expansions_per_launch": expanded_per_step,
-                                    "peak_source": "nominal 148 SM x 128 B/clk at the sampled SM clock"}},
+            "roofline": roofline,
             "cpu_baseline": cpu,
             "plain": plain,
             "clocks": clk,
@@ -469,14 +560,96 @@ def run_sbfs(args):
                         "max_length": int(lens.max()) if count else 0},
             "plan": plan,
         }
-        if serving:
-            line["serving"] = serving
-        print(json.dumps(line), flush=True)
+        if args.workload == "n12" and world == 1:
+            if not args.no_serving:
+                def brief(e):
+                    return {"offered_per_s": e["offered_per_s"], "achieved_per_s": e["achieved_automata_per_s"],
+                            "p50_ms_n_le_20": e["latency_ms_n_le_20"]["p50"],
+                            "p99_ms_n_le_20": e["latency_ms_n_le_20"]["p99"],
+                            "p99_ms_all": e["latency_ms"]["p99"]}
+                line["serving"] = {"requests": 10_000,
+                                   "sweep": [brief(e) for e in serve_sweep(10_000, [32000.0, 0.0])],
+                                   "full_sweep": "bench.py --workload serving"}
+            if not args.no_extra:
+                line.update(extra_summaries(args, eng, dev, stream, flush, hbm_peak, threads))
     eng.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
     return 0
+
+
+def extra_summaries(args, eng, dev, stream, flush, hbm_peak: float, threads: int) -> dict:
+    """The other configurations, each device-timed (L2 flushed before every
+    step) with its CPU restatement beside it and its lengths compared with it."""
+    import numpy as np
+    import torch
+    out = {}
+    steps, warm = max(args.extra_steps, 1), 3
+
+    def cpu_leg(wl):
+        t0 = time.perf_counter()
+        r, kind = cpu_pass(wl, threads, lengths=True)
+        dt = time.perf_counter() - t0
+        return r["len"], {"value": wl["count"] / dt, "unit": UNIT, "cores": threads, "kind": "port",
+                          "sample": f"one pass over the {wl['count']:,} automata ({kind})"}
+
+    # config 3: 200K automata, n uniform 6..20, 1 % Cerny
+    wl = make_workload("mixed")
+    leg = DeviceLeg(eng, wl, dev, stream)
+    ms_l, st, _ = leg.timed(steps, warm, flush)
+    ms = statistics.mean(ms_l)
+    ref, cpu = cpu_leg(wl)
+    out["mixed"] = {"workload": wl["desc"], "ms_per_step": ms, "automata_per_s": wl["count"] / (ms / 1e3),
+                    "expansions_per_step": int(st["expanded"]), "gpu_launches_per_step": int(st["launches"]),
+                    "lengths_match_cpu": bool(np.array_equal(leg.d_len.cpu().numpy(), ref)),
+                    "cpu_baseline": cpu, "steps": steps}
+    del leg
+
+    # config 5: n = 24, 26, 28 x (64 random + C_n + permutation-plus-merge)
+    wl = make_workload("large")
+    leg = DeviceLeg(eng, wl, dev, stream)
+    ms_l, st, _ = leg.timed(max(2, steps // 2), 2, flush)
+    ms = statistics.mean(ms_l)
+    search = int(st["expanded"]) * LEVEL_BYTES_PER_EXPANSION
+    gbs = search / (ms / 1e3) / 1e9
+    ref, cpu = cpu_leg(wl)
+    out["large"] = {"workload": wl["desc"], "ms_per_step": ms, "automata_per_s": wl["count"] / (ms / 1e3),
+                    "expansions_per_step": int(st["expanded"]),
+                    "hbm_search": {"achieved": gbs, "peak": hbm_peak, "unit": "GB/s", "frac": gbs / hbm_peak,
+                                   "algorithmic_bytes": f"{LEVEL_BYTES_PER_EXPANSION} B per expansion"},
+                    "lengths_match_cpu": bool(np.array_equal(leg.d_len.cpu().numpy(), ref)),
+                    "cpu_baseline": cpu, "steps": max(2, steps // 2)}
+    del leg
+
+    # the reference's published configuration: n = 13, batch 2^21 (System.Random)
+    wl = make_workload("n13")
+    leg = DeviceLeg(eng, wl, dev, stream)
+    ms_l, st, _ = leg.timed(steps, warm, flush)
+    ms = statistics.mean(ms_l)
+    dev_len = leg.d_len.cpu().numpy()
+    del leg
+    # end to end as the reference times it: one Verify call (lengths only) on host buffers
+    eng.verify(wl["recs"], n=13, lstride=13)
+    v_ms = []
+    for i in range(steps):
+        flush.fill_(i)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rv = eng.verify(wl["recs"], n=13, lstride=13)
+        v_ms.append((time.perf_counter() - t0) * 1e3)
+    ref, cpu = cpu_leg(wl)
+    vm = statistics.mean(v_ms)
+    out["n13"] = {"workload": wl["desc"], "seed": wl["seed"], "ms_per_step": ms,
+                  "automata_per_s": wl["count"] / (ms / 1e3),
+                  "verify_e2e": {"value": wl["count"] / (vm / 1e3), "unit": UNIT, "ms_per_step": vm,
+                                 "what": "sbfs_verify_batch on host buffers (lengths only), as Program.cs:111 "
+                                         "times IComputable.Verify"},
+                  "lengths_match_cpu": bool(np.array_equal(dev_len, ref) and np.array_equal(rv["len"], ref)),
+                  "cpu_baseline": cpu, "published": PUBLISHED_N13, "steps": steps}
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -591,8 +764,11 @@ def run_serving(args):
     return 0
 
 
-def main():
-    args = parse_args()
+def main(argv=None):
+    argv = sys.argv[1:] if argv is None else argv
+    args = parse_args(argv)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return self_launch(args, argv)
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "serving":

@@ -16,6 +16,7 @@
 #include <chrono>
 #include <climits>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <thread>
@@ -692,6 +693,7 @@ sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstr
         CK(cudaMemcpyAsync(L.maps.as<uint8_t>() + a * rec, src + a * rec, m * rec, cudaMemcpyHostToDevice,
                            h->copy_in),
            "copying records");
+        if (ci == h->skip_ready_chunk) return SBFS_OK;   // test hook: this chunk's flag never comes
         CK(cudaMemcpyAsync(ready + ci, hf + 2 * nch + ci, sizeof(unsigned int), cudaMemcpyHostToDevice, h->copy_in),
            "setting a chunk flag");
         return SBFS_OK;
@@ -720,7 +722,8 @@ sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstr
     b.first_violation = &ctr->first_violation;
     b.expanded = &ctr->expanded;
     b.error = &ctr->error;
-    LaneStream lsd{ready, done, d_host_flag, kStreamChunk, S.escal_out.as<EscalResult>()};
+    LaneStream lsd{ready, done, d_host_flag, kStreamChunk, S.escal_out.as<EscalResult>(),
+                   h->cfg.wait_polls > 0 ? h->cfg.wait_polls : (1 << 24)};
     CK(cudaEventRecord(L.ev_k0, L.stream), "recording event");
     CK(launch_lane(ls.nmax, ls.warps, ls.ring, ls.refill_k, ls.tail_k, ls.ctas, b, L.escal.as<int32_t>(),
                    (unsigned long long)cnt, &ctr->escal_count[c], &ctr->escal_claim[c], &ctr->ticket[c], lsd,
@@ -857,6 +860,7 @@ sbfs_status solve_host(sbfs_handle *h, const uint8_t *maps, int32_t lstride, con
             so.first_violation =
                 fv_before >= 0 ? fv_before : (so.first_violation >= 0 ? begin + so.first_violation : -1);
         }
+        h->skip_ready_chunk = -1;   // the test hook is one-shot
         if (out_first_violation) *out_first_violation = so.first_violation;
         if (stats) {
             stats->automata = count;
@@ -1108,6 +1112,7 @@ sbfs_status sbfs_create(const sbfs_config *cfg, sbfs_handle **out)
     h->sm_count = prop.multiProcessorCount;
     h->smem_optin = prop.sharedMemPerBlockOptin;
     h->cfg = c;
+    if (const char *skip = std::getenv("SBFS_TEST_SKIP_CHUNK_READY")) h->skip_ready_chunk = std::atoll(skip);
     h->lanes.resize(c.streams > 0 ? std::min(c.streams, 16) : kDefaultLanes);
     if ((e = cudaEventCreateWithFlags(&h->ev_device, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreate(&h->ev_dk0)) != cudaSuccess || (e = cudaEventCreate(&h->ev_dk1)) != cudaSuccess ||

@@ -135,6 +135,7 @@ struct LaneStream {
     unsigned int *host_flag;           // mapped host memory: 1 once chunk c's outcomes are all written
     int64_t chunk;                     // automata per chunk (records of a chunk fill whole 128-byte lines)
     EscalResult *escal_out;            // by escalation slot: results the whole-warp search writes
+    int wait_polls;                    // bounded wait for a chunk's records: polls before giving up
 };
 
 // Stores the first *count escalated results into device-accessible (e.g.

@@ -105,10 +105,11 @@ __device__ int64_t claim_escalated(int32_t *list, unsigned long long capacity, u
     return prev >= 0 ? (int64_t)prev : -1;
 }
 
-// Waits (bounded) until the streamed records of chunk c are on the device.
-__device__ bool wait_chunk(const unsigned int *ready, int64_t c)
+// Waits (bounded: `polls` polls about 0.2 us apart) until the streamed records
+// of chunk c are on the device; false when the wait ran out.
+__device__ bool wait_chunk(const unsigned int *ready, int64_t c, int polls)
 {
-    for (int it = 0; it < (1 << 24); ++it) {
+    for (int it = 0; it < polls; ++it) {
         if (*(volatile const unsigned int *)(ready + c)) {
             __threadfence();
             return true;
@@ -325,7 +326,7 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
                     const int64_t c_last = last / ls.chunk;
                     if (c_last > ready_upto) {
                         bool ok = true;
-                        if (lane == 0) ok = wait_chunk(ls.chunk_ready, c_last);
+                        if (lane == 0) ok = wait_chunk(ls.chunk_ready, c_last, ls.wait_polls);
                         ok = __shfl_sync(kFull, ok, 0);
                         if (!ok && lane == 0) atomicOr(b.error, kErrWait);
                         ready_upto = c_last;

@@ -19,10 +19,13 @@
 //    makes this path slower than sbfs_solve_batch_device.
 //  * Every call uses the same array; calls that overlap on the GPU race with
 //    each other.  Serialise them (one stream, or events between streams).
-//  * The first call on a device looks up the array's device address with
-//    cudaGetSymbolAddress (once per device, with that device current); make
-//    that first call before any stream capture begins.
-#include <mutex>
+//  * Every call looks up the array's device address on the current device
+//    with cudaGetSymbolAddress (no allocation), so a new context after a
+//    device reset gets the array's new address.  The first call on a device
+//    may load the library's device code there; make it before any stream
+//    capture begins.
+//  * d_len is required: a malformed record (a state index >= n) is reported
+//    only through its length, -2.
 
 #include "common.cuh"
 
@@ -31,7 +34,6 @@ namespace {
 
 constexpr size_t kScratchBytes = size_t(16) << 20;
 constexpr size_t kHeaderBytes = 256;
-constexpr int kMaxDevices = 64;
 
 struct NoAllocHeader {
     unsigned long long ticket;
@@ -44,9 +46,6 @@ static_assert(sizeof(NoAllocHeader) <= kHeaderBytes, "header");
 // The working memory of every call (header, then the queue spill area).
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
-std::mutex g_mu;
-unsigned char *g_scratch_ptr[kMaxDevices] = {};
-
 // Pooled-kernel shape: 4 automata per warp, 2 warps per CTA, 256 queue
 // entries on chip; each slot spills at most 2^12 - 256 entries (15 KiB).
 constexpr int kNmax = 12, kSlots = 4, kWarps = 2, kQueueSmem = 256;
@@ -58,21 +57,16 @@ __global__ void finalize(const NoAllocHeader *hdr, int64_t *out)
     *out = hdr->first_violation == ~0ull ? -1ll : (int64_t)hdr->first_violation;
 }
 
-// Device address of g_scratch for the current device (set up once per device).
+// Device address of g_scratch in the current device's context.  In host code
+// the name g_scratch is a host-side stand-in, not a device address; it is
+// looked up on every call, so a context created after a device reset is
+// served at the array's new address.
 cudaError_t scratch_address(unsigned char **out)
 {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_ptr[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_scratch);
-        if (e != cudaSuccess) return e;
-        g_scratch_ptr[dev] = static_cast<unsigned char *>(p);
-    }
-    *out = g_scratch_ptr[dev];
+    *out = static_cast<unsigned char *>(p);
     return cudaSuccess;
 }
 
@@ -85,7 +79,8 @@ extern "C" sbfs_status sbfs_solve_small_noalloc(const uint8_t *d_maps, int32_t l
 {
     using namespace sbfs;
     if (n < 1 || n > kNmax) return SBFS_EINVAL;   // beyond what the static scratch holds
-    if (lstride < n || lstride > 32 || count < 0 || (count > 0 && !d_maps) || !d_first_violation)
+    if (lstride < n || lstride > 32 || count < 0 || (count > 0 && !d_maps) || !d_first_violation ||
+        (count > 0 && !d_len))
         return SBFS_EINVAL;
     if (d_words && word_stride < 1) return SBFS_EINVAL;
     unsigned char *scratch = nullptr;

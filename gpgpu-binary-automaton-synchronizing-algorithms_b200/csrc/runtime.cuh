@@ -189,4 +189,8 @@ struct sbfs_handle {
     int64_t device_count = 0;
     int device_launches = 0;
     cudaEvent_t ev_dk0 = nullptr, ev_dk1 = nullptr;
+    // host-side fault injection for tests (environment SBFS_TEST_SKIP_CHUNK_READY=c
+    // at sbfs_create): the next streamed call never sets chunk c's ready flag,
+    // so the kernel's bounded wait for it runs out; then the hook is cleared
+    int64_t skip_ready_chunk = -1;
 };

@@ -24,6 +24,7 @@
 // Completion order follows the GPU, not submission order.
 #include <atomic>
 #include <chrono>
+#include <cstdlib>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -56,6 +57,7 @@ struct SmallSlot {
     DevBuf d_recs, d_ns;
     HostBuf h_recs, h_ns;                // staging in
     HostBuf h_len, h_words, h_flags;     // mapped: the kernels store results and flags here
+    HostBuf h_err;                       // the launch set's device error word, copied back behind it
     int32_t *dl = nullptr;               // device aliases of the mapped buffers
     uint64_t *dw = nullptr;
     unsigned int *df = nullptr;
@@ -63,6 +65,7 @@ struct SmallSlot {
     std::vector<char> delivered;
     size_t left = 0;                     // requests not yet delivered
     unsigned int tag = 0;                // this launch's flag value
+    int64_t seq = 0;                     // 1-based launch number of the mini-batch
     cudaEvent_t ev = nullptr;
     bool busy = false;
 };
@@ -92,6 +95,15 @@ struct sbfs_server {
     LevelEngine big;                               // level slots for n >= 21
     std::unordered_map<long long, Request> large;   // admitted, keyed by id
     std::string error;
+    // set once a CUDA call of the loop failed: every request still held, and
+    // every later one, completes with failed_status (the context may be lost)
+    bool failed = false;
+    int32_t failed_status = SBFS_ECUDA;
+    int64_t batches_launched = 0;
+    // host-side fault injection for tests (environment SBFS_SERVER_FAIL_BATCH=k):
+    // mini-batch k is reported as failed once its work has completed, as a
+    // failed cudaEventQuery would report it; no GPU fault is involved
+    int64_t inject_fail_batch = 0;
 
     double now_ms() const
     {
@@ -119,7 +131,9 @@ void complete(sbfs_server *s, const Request &r, int32_t status, int32_t len, con
     s->cv_out.notify_all();
 }
 
-bool event_done(cudaEvent_t ev);
+enum class Ev { kPending, kDone, kFailed };
+Ev event_state(cudaEvent_t ev, cudaError_t *err);
+void fail_all(sbfs_server *s, int32_t status, const std::string &why);
 
 bool launch_small(sbfs_server *s, SmallSlot &S)
 {
@@ -157,28 +171,62 @@ bool launch_small(sbfs_server *s, SmallSlot &S)
         S.reqs.clear();
         return false;
     }
-    cudaEventRecord(S.ev, st);
+    // the launch set's error bits come back behind its kernels, before the event
+    cudaError_t ce = cudaMemcpyAsync(S.h_err.ptr, &L.counters.as<DevCounters>()->error, sizeof(int),
+                                     cudaMemcpyDeviceToHost, st);
+    if (ce == cudaSuccess) ce = cudaEventRecord(S.ev, st);
+    if (ce != cudaSuccess) {
+        cudaGetLastError();
+        S.delivered.assign((size_t)cnt, 0);
+        S.left = (size_t)cnt;
+        S.busy = true;   // fail_all completes this slot's requests
+        fail_all(s, SBFS_ECUDA, std::string("serving: ") + cudaGetErrorString(ce));
+        return true;
+    }
     S.delivered.assign((size_t)cnt, 0);
     S.left = (size_t)cnt;
     S.busy = true;
+    S.seq = ++s->batches_launched;
     std::lock_guard<std::mutex> lock(s->mu);
     s->st.small_batches++;
     return true;
 }
 
 // Delivers the slot's requests whose flags are up; frees the slot once its
-// launch sequence has completed.
+// launch sequence has completed.  A launch set that failed (a CUDA error on
+// its stream, or error bits in its device error word) completes its requests
+// not yet delivered with an error status, never with stale results.
 bool poll_small(sbfs_server *s, SmallSlot &S)
 {
     bool progress = false;
     const volatile unsigned int *flag = S.h_flags.as<unsigned int>();
     const int32_t *len = S.h_len.as<int32_t>();
     const uint64_t *words = S.h_words.as<uint64_t>();
-    const bool finished = event_done(S.ev);   // sampled before the flags: all are up once it is done
+    cudaError_t err = cudaSuccess;
+    Ev ev = event_state(S.ev, &err);   // sampled before the flags: all are up once it is done
+    if (ev == Ev::kDone && S.seq == s->inject_fail_batch) {
+        ev = Ev::kFailed;
+        err = cudaErrorLaunchFailure;
+    }
+    if (ev == Ev::kFailed) {
+        fail_all(s, SBFS_ECUDA, std::string("serving mini-batch: ") + cudaGetErrorString(err));
+        return true;
+    }
+    const bool finished = ev == Ev::kDone;
+    int32_t status = SBFS_OK;
+    if (finished) {
+        const int bits = *(volatile const int *)S.h_err.ptr;
+        if (bits) {
+            status = (bits & kErrInvalid) ? SBFS_EINVAL : SBFS_ECUDA;
+            s->error = (bits & kErrInvalid) ? "serving mini-batch: malformed automaton"
+                                            : "serving mini-batch: device error bits set";
+        }
+    }
     for (size_t i = 0; i < S.reqs.size() && S.left; ++i) {
         if (S.delivered[i] || (flag[i] != S.tag && !finished)) continue;
         std::atomic_thread_fence(std::memory_order_acquire);
-        complete(s, S.reqs[i], SBFS_OK, len[i], words + i * kWords);
+        if (status == SBFS_OK) complete(s, S.reqs[i], SBFS_OK, len[i], words + i * kWords);
+        else complete(s, S.reqs[i], status, -1, nullptr);
         S.delivered[i] = 1;
         --S.left;
         progress = true;
@@ -233,14 +281,40 @@ cudaError_t prime_small(sbfs_server *s)
     return cudaSuccess;
 }
 
-bool event_done(cudaEvent_t ev)
+// cudaEventQuery as done / pending / failed: anything but success and
+// cudaErrorNotReady is a failure of the work before the event.
+Ev event_state(cudaEvent_t ev, cudaError_t *err)
 {
     const cudaError_t e = cudaEventQuery(ev);
-    if (e == cudaErrorNotReady) {
-        cudaGetLastError();
-        return false;
+    if (e == cudaSuccess) return Ev::kDone;
+    cudaGetLastError();
+    if (e == cudaErrorNotReady) return Ev::kPending;
+    *err = e;
+    return Ev::kFailed;
+}
+
+// Completes every request the loop holds (mini-batches in flight, admitted and
+// waiting large requests, pending small ones) with `status`, and every later
+// request too: after a failed CUDA call the loop launches nothing more.
+void fail_all(sbfs_server *s, int32_t status, const std::string &why)
+{
+    if (!s->failed) s->error = why;
+    s->failed = true;
+    s->failed_status = status;
+    for (SmallSlot &S : s->small) {
+        if (!S.busy) continue;
+        for (size_t i = 0; i < S.reqs.size(); ++i)
+            if (!S.delivered[i]) complete(s, S.reqs[i], status, -1, nullptr);
+        S.reqs.clear();
+        S.left = 0;
+        S.busy = false;
     }
-    return true;
+    for (auto &kv : s->large) complete(s, kv.second, status, -1, nullptr);
+    s->large.clear();
+    for (const Request &r : s->pend_small) complete(s, r, status, -1, nullptr);
+    for (const Request &r : s->pend_big) complete(s, r, status, -1, nullptr);
+    s->pend_small.clear();
+    s->pend_big.clear();
 }
 
 void run_loop(sbfs_server *s)
@@ -272,25 +346,31 @@ void run_loop(sbfs_server *s)
                 progress = true;
             }
         }
+        if (s->failed) {
+            // nothing more is launched: what arrives completes with the failure status
+            fail_all(s, s->failed_status, s->error);
+        }
         // small path
         for (SmallSlot &S : s->small)
             if (S.busy) progress |= poll_small(s, S);
         for (SmallSlot &S : s->small)
-            if (!S.busy && !s->pend_small.empty()) progress |= launch_small(s, S);
+            if (!s->failed && !S.busy && !s->pend_small.empty()) progress |= launch_small(s, S);
         // large path
         LevelEngine &E = s->big;
-        if (E.launched() && E.ready()) {
+        if (!s->failed && E.launched() && E.ready()) {
             fin.clear();
-            E.collect(fin);
+            const cudaError_t ce = E.collect(fin);
             for (auto &f : fin) {
                 auto it = s->large.find(f.tag);
                 if (it == s->large.end()) continue;
                 complete(s, it->second, f.state == kSlotDone ? SBFS_OK : SBFS_ECUDA, f.len, f.word);
                 s->large.erase(it);
             }
+            if (ce != cudaSuccess) fail_all(s, SBFS_ECUDA, std::string("serving level slots: ") +
+                                                               cudaGetErrorString(ce));
             progress = true;
         }
-        if (!E.launched()) {
+        if (!s->failed && !E.launched()) {
             while (!s->pend_big.empty()) {
                 const Request &r = s->pend_big.front();
                 if (E.admit(nullptr, 32, r.n, (long long)r.id, r.a, r.b) < 0) break;
@@ -298,9 +378,14 @@ void run_loop(sbfs_server *s)
                 s->pend_big.pop_front();
             }
             if (E.in_flight() > 0) {
-                E.launch(s->cfg.max_levels, none, 4 * s->cfg.max_levels);
-                std::lock_guard<std::mutex> lock(s->mu);
-                s->st.level_launches += s->cfg.max_levels;
+                const cudaError_t ce = E.launch(s->cfg.max_levels, none, 4 * s->cfg.max_levels);
+                if (ce != cudaSuccess) {
+                    cudaGetLastError();
+                    fail_all(s, SBFS_ECUDA, std::string("serving level launch: ") + cudaGetErrorString(ce));
+                } else {
+                    std::lock_guard<std::mutex> lock(s->mu);
+                    s->st.level_launches += s->cfg.max_levels;
+                }
                 progress = true;
             }
         }
@@ -354,6 +439,7 @@ sbfs_status sbfs_server_start(const sbfs_server_config *cfg, sbfs_server **out)
     if (s->cfg.max_levels <= 0) s->cfg.max_levels = 16;
     if (s->cfg.queue_capacity <= 0) s->cfg.queue_capacity = 1 << 20;
     if (s->cfg.arena_bytes <= 0) s->cfg.arena_bytes = (int64_t)16 << 30;
+    if (const char *inj = std::getenv("SBFS_SERVER_FAIL_BATCH")) s->inject_fail_batch = std::atoll(inj);
     sbfs_config hc;
     sbfs_config_default(&hc);
     hc.device = s->cfg.device;
@@ -371,7 +457,8 @@ sbfs_status sbfs_server_start(const sbfs_server_config *cfg, sbfs_server **out)
         S.lane = i;
         if ((e = S.d_recs.reserve(mb * 64)) || (e = S.d_ns.reserve(mb)) || (e = S.h_recs.reserve(mb * 64)) ||
             (e = S.h_ns.reserve(mb)) || (e = S.h_len.reserve(mb * 4)) || (e = S.h_words.reserve(mb * kWords * 8)) ||
-            (e = S.h_flags.reserve(mb * 4)) || (e = cudaHostGetDevicePointer((void **)&S.dl, S.h_len.ptr, 0)) ||
+            (e = S.h_flags.reserve(mb * 4)) || (e = S.h_err.reserve(sizeof(int))) ||
+            (e = cudaHostGetDevicePointer((void **)&S.dl, S.h_len.ptr, 0)) ||
             (e = cudaHostGetDevicePointer((void **)&S.dw, S.h_words.ptr, 0)) ||
             (e = cudaHostGetDevicePointer((void **)&S.df, S.h_flags.ptr, 0)) ||
             (e = cudaEventCreateWithFlags(&S.ev, cudaEventDisableTiming)))
@@ -388,7 +475,7 @@ sbfs_status sbfs_server_start(const sbfs_server_config *cfg, sbfs_server **out)
         for (SmallSlot &S : s->small) {
             if (S.ev) cudaEventDestroy(S.ev);
             for (DevBuf *d : {&S.d_recs, &S.d_ns}) d->release();
-            for (HostBuf *b : {&S.h_recs, &S.h_ns, &S.h_len, &S.h_words, &S.h_flags}) b->release();
+            for (HostBuf *b : {&S.h_recs, &S.h_ns, &S.h_len, &S.h_words, &S.h_flags, &S.h_err}) b->release();
         }
         sbfs_destroy(s->h);
         delete s;
@@ -490,7 +577,7 @@ sbfs_status sbfs_server_stop(sbfs_server *s)
     for (SmallSlot &S : s->small) {
         if (S.ev) cudaEventDestroy(S.ev);
         for (DevBuf *d : {&S.d_recs, &S.d_ns}) d->release();
-        for (HostBuf *b : {&S.h_recs, &S.h_ns, &S.h_len, &S.h_words, &S.h_flags}) b->release();
+        for (HostBuf *b : {&S.h_recs, &S.h_ns, &S.h_len, &S.h_words, &S.h_flags, &S.h_err}) b->release();
     }
     sbfs_destroy(s->h);
     delete s;

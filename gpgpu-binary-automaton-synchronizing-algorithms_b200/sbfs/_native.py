@@ -59,6 +59,7 @@ class Config(ctypes.Structure):
         ("streams", ctypes.c_int32),
         ("level_arena_bytes", ctypes.c_int64),
         ("tune_cache", ctypes.c_char_p),
+        ("wait_polls", ctypes.c_int32),
     ]
 
 

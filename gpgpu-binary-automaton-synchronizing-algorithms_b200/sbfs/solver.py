@@ -40,7 +40,7 @@ class Engine:
                  slots_per_warp: int = 0, warps_per_cta: int = 0, queue_smem: int = 0, chunk: int = 0,
                  small_kernel: int = 0, lane_ring: int = 0, lane_refill: int = 0, lane_warps: int = 0,
                  lane_tail: int = 0, streams: int = 0,
-                 level_arena_bytes: int = 0, tune_cache: Optional[str] = None):
+                 level_arena_bytes: int = 0, tune_cache: Optional[str] = None, wait_polls: int = 0):
         self.lib = _native.load()
         cfg = _native.Config()
         self.lib.sbfs_config_default(ctypes.byref(cfg))
@@ -61,6 +61,7 @@ class Engine:
         cfg.level_arena_bytes = level_arena_bytes
         self._tune_cache = tune_cache.encode() if tune_cache else None
         cfg.tune_cache = self._tune_cache
+        cfg.wait_polls = wait_polls
         h = ctypes.c_void_p()
         st = self.lib.sbfs_create(ctypes.byref(cfg), ctypes.byref(h))
         if st != 0:

@@ -57,7 +57,7 @@ extern "C" {
 #endif
 
 #define SBFS_MAX_N 28
-#define SBFS_ABI_VERSION 1
+#define SBFS_ABI_VERSION 2
 
 typedef enum sbfs_status {
     SBFS_OK = 0,
@@ -97,6 +97,9 @@ typedef struct sbfs_config {
     int32_t streams;           /* streams the host path rotates chunks over; 0 = 4      */
     int64_t level_arena_bytes; /* HBM budget of the n > 20 level slots; 0 = half of free memory, <= 64 GiB */
     const char *tune_cache;    /* autotuner cache file, or NULL for in-memory only      */
+    int32_t wait_polls;        /* device-side bounded waits (the streamed host path's wait for a
+                                  chunk of records): polls of about 0.2 us before the kernel gives
+                                  up and the call returns SBFS_ETIMEOUT; 0 = 2^24 (ABI version 2) */
 } sbfs_config;
 
 typedef struct sbfs_stats {
@@ -184,10 +187,12 @@ SBFS_API sbfs_status sbfs_host_free(void *p);
  * enqueued on `stream` (a cudaStream_t; NULL = the default stream), and keeps
  * all of its working memory in one fixed 16 MiB array inside the library.
  * n > 12 returns SBFS_EINVAL.  Every call shares that array, so calls that
- * overlap on the GPU race; serialise them.  The first call on a device looks
- * the array up (cudaGetSymbolAddress); make it before any stream capture.
- * A malformed record gets length -2 in d_len.  Words and lengths follow the
- * conventions above; it is slower than sbfs_solve_batch_device.
+ * overlap on the GPU race; serialise them.  Every call looks the array up
+ * in the current context (cudaGetSymbolAddress, which allocates nothing); the
+ * first call on a device may load the library's device code, so make it
+ * before any stream capture.  d_len is required (SBFS_EINVAL without it): a
+ * malformed record is reported only as length -2 there.  Words and lengths
+ * follow the conventions above; it is slower than sbfs_solve_batch_device.
  */
 SBFS_API sbfs_status sbfs_solve_small_noalloc(const uint8_t *d_maps, int32_t lstride, int32_t n,
                                               int64_t count, int32_t *d_len, uint64_t *d_words,

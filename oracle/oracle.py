@@ -42,6 +42,11 @@ def lib():
         L.orc_replay.argtypes = [P, ctypes.c_int, P, ctypes.c_int, ctypes.c_int64, P, P,
                                  ctypes.c_int, P]
         L.orc_replay.restype = ctypes.c_int64
+        L.orc_fill_array_of_problems.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.c_int32, P,
+                                                 ctypes.c_int, ctypes.c_int]
+        L.orc_fill_array_of_problems.restype = ctypes.c_int
+        L.orc_dotnet_random_next.argtypes = [ctypes.c_int32, ctypes.c_int32, P]
+        L.orc_dotnet_random_next.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -102,3 +107,26 @@ def replay(recs: np.ndarray, lens: np.ndarray, words: np.ndarray, ns=None, n: in
     bad = lib().orc_replay(_ptr(recs), lstride, _ptr(ns_arr), int(n), recs.shape[0],
                            _ptr(lens), _ptr(words), words.shape[1], _ptr(ok))
     return int(bad), ok
+
+
+def fill_array_of_problems(count: int, n: int, seed: int, lstride: int = 32, threads: int = 1) -> np.ndarray:
+    """Problem.FillArrayOfProblems (SharedDefinitions/Problem.cs:32-58) with
+    .NET System.Random, as records of 2*lstride bytes (a = rec[:n],
+    b = rec[lstride:lstride + n]); the CPU legs build the reference's batches
+    with it so that they never load the product library."""
+    count, n, lstride = int(count), int(n), int(lstride)
+    out = np.empty((count, 2 * lstride), dtype=np.uint8)
+    st = lib().orc_fill_array_of_problems(count, n, int(seed), _ptr(out) if count else None, lstride,
+                                          int(threads))
+    if st != 0:
+        raise ValueError(f"oracle orc_fill_array_of_problems failed with status {st}")
+    return out
+
+
+def dotnet_random_next(seed: int, count: int) -> np.ndarray:
+    """The first ``count`` values of ``new System.Random(seed).Next()``."""
+    out = np.empty(int(count), dtype=np.int32)
+    st = lib().orc_dotnet_random_next(int(seed), int(count), _ptr(out) if count else None)
+    if st != 0:
+        raise ValueError(f"oracle orc_dotnet_random_next failed with status {st}")
+    return out

@@ -21,6 +21,10 @@
  *                  reference's timed Verify mode (lengths optional).
  *   orc_replay     Verify.VerifyValidityOfSynchronizingWord and
  *                  VerifyCernyConjecture (GPGPU/Result veryfier/Verify.cs:12-62).
+ *   orc_fill_array_of_problems
+ *                  Problem.FillArrayOfProblems (SharedDefinitions/Problem.cs:32-58)
+ *                  with .NET Framework's System.Random, so that the CPU baseline
+ *                  builds the reference's own batches without the product library.
  *
  * Automaton record layout (shared with the CUDA library): record i occupies
  * 2*lstride bytes at maps + i*2*lstride; a[j] = rec[j], b[j] = rec[lstride + j].
@@ -401,4 +405,125 @@ int64_t orc_replay(const uint8_t *maps, int lstride, const uint8_t *ns, int n_un
         if (ok != 3) ++bad;
     }
     return bad;
+}
+
+/* ---------------------------------------------------------------------------
+ * .NET Framework System.Random: Knuth's subtractive generator (TAOCP vol. 2,
+ * 3.6), as .NET seeds it: a 55-entry table filled at stride 21 from
+ * 161803398 - |seed|, stirred four times, outputs taken as differences at lags
+ * 55 and 34 modulo 2^31 - 1.  C# int arithmetic is unchecked, so differences
+ * wrap in two's complement (seeds above 161803398 make that happen).
+ * ------------------------------------------------------------------------- */
+typedef struct {
+    int32_t t[56];
+    int inext, inextp;
+} orc_dotnet_random;
+
+static inline int32_t orc_wrap_sub(int32_t a, int32_t b)
+{
+    return (int32_t)((uint32_t)a - (uint32_t)b);
+}
+
+static void orc_random_seed(orc_dotnet_random *r, int32_t seed)
+{
+    const int32_t big = 2147483647, mseed = 161803398;
+    const int32_t sub = seed == INT32_MIN ? big : (seed < 0 ? -seed : seed);
+    int32_t mj = orc_wrap_sub(mseed, sub), mk = 1;
+    memset(r->t, 0, sizeof(r->t));
+    r->t[55] = mj;
+    for (int i = 1; i < 55; ++i) {
+        const int ii = (21 * i) % 55;
+        r->t[ii] = mk;
+        mk = orc_wrap_sub(mj, mk);
+        if (mk < 0) mk += big;
+        mj = r->t[ii];
+    }
+    for (int pass = 0; pass < 4; ++pass)
+        for (int i = 1; i < 56; ++i) {
+            r->t[i] = orc_wrap_sub(r->t[i], r->t[1 + (i + 30) % 55]);
+            if (r->t[i] < 0) r->t[i] += big;
+        }
+    r->inext = 0;
+    r->inextp = 21;
+}
+
+static int32_t orc_random_next(orc_dotnet_random *r)   /* Random.Next(): [0, 2^31 - 1) */
+{
+    const int32_t big = 2147483647;
+    if (++r->inext >= 56) r->inext = 1;
+    if (++r->inextp >= 56) r->inextp = 1;
+    int32_t v = orc_wrap_sub(r->t[r->inext], r->t[r->inextp]);
+    if (v == big) --v;
+    if (v < 0) v += big;
+    r->t[r->inext] = v;
+    return v;
+}
+
+static int32_t orc_random_range(orc_dotnet_random *r, int32_t lo, int32_t hi)   /* Random.Next(lo, hi) */
+{
+    const double sample = orc_random_next(r) * (1.0 / 2147483647.0);
+    return (int32_t)(sample * (double)((int64_t)hi - lo)) + lo;
+}
+
+typedef struct {
+    const int32_t *seeds;
+    uint8_t *maps;
+    int n, lstride;
+    int64_t begin, end;
+} orc_fill_job;
+
+static void *orc_fill_slice(void *arg)
+{
+    orc_fill_job *j = (orc_fill_job *)arg;
+    orc_dotnet_random r;
+    for (int64_t p = j->begin; p < j->end; ++p) {
+        uint8_t *rec = j->maps + (size_t)p * 2 * (size_t)j->lstride;
+        orc_random_seed(&r, j->seeds[p]);                 /* GenerateProblem(n, seed), Problem.cs:41-58 */
+        memset(rec, 0, 2 * (size_t)j->lstride);
+        for (int i = 0; i < j->n; ++i) {                  /* A[i] then B[i], Problem.cs:52-56 */
+            rec[i] = (uint8_t)orc_random_range(&r, 0, j->n);
+            rec[j->lstride + i] = (uint8_t)orc_random_range(&r, 0, j->n);
+        }
+    }
+    return NULL;
+}
+
+/* FillArrayOfProblems(problems, count, n, seed) (Problem.cs:32-39) into records
+ * of 2*lstride bytes, bytes past n zero; the per-automaton generators run on
+ * `threads` threads (the master stream is sequential). */
+int orc_fill_array_of_problems(int64_t count, int n, int32_t seed, uint8_t *maps, int lstride, int threads)
+{
+    if (count < 0 || n < 1 || n > 28 || lstride < n || lstride > 32 || (count > 0 && !maps)) return ORC_EINVAL;
+    if (count == 0) return ORC_OK;
+    int32_t *seeds = (int32_t *)malloc((size_t)count * sizeof(int32_t));
+    if (!seeds) return ORC_ENOMEM;
+    orc_dotnet_random master;
+    orc_random_seed(&master, seed);
+    for (int64_t p = 0; p < count; ++p) seeds[p] = orc_random_next(&master);   /* Problem.cs:37 */
+    if (threads < 1) threads = 1;
+    if (threads > count) threads = (int)count;
+    orc_fill_job *jobs = (orc_fill_job *)calloc((size_t)threads, sizeof(orc_fill_job));
+    pthread_t *tid = (pthread_t *)calloc((size_t)threads, sizeof(pthread_t));
+    if (!jobs || !tid) { free(jobs); free(tid); free(seeds); return ORC_ENOMEM; }
+    const int64_t part = (count + threads - 1) / threads;
+    for (int t = 0; t < threads; ++t) {
+        jobs[t].seeds = seeds; jobs[t].maps = maps; jobs[t].n = n; jobs[t].lstride = lstride;
+        jobs[t].begin = (int64_t)t * part < count ? (int64_t)t * part : count;
+        jobs[t].end = (int64_t)(t + 1) * part < count ? (int64_t)(t + 1) * part : count;
+    }
+    for (int t = 1; t < threads; ++t) pthread_create(&tid[t], NULL, orc_fill_slice, &jobs[t]);
+    orc_fill_slice(&jobs[0]);
+    for (int t = 1; t < threads; ++t) pthread_join(tid[t], NULL);
+    free(jobs); free(tid); free(seeds);
+    return ORC_OK;
+}
+
+/* The first count values of new System.Random(seed).Next(). */
+int orc_dotnet_random_next(int32_t seed, int32_t count, int32_t *out)
+{
+    if (count < 0 || (count > 0 && !out)) return ORC_EINVAL;
+    orc_dotnet_random r;
+    orc_random_seed(&r, seed);
+    for (int32_t i = 0; i < count; ++i) out[i] = orc_random_next(&r);
+    return ORC_OK;
 }

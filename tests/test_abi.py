@@ -40,7 +40,7 @@ def test_binding_list_covers_header():
 
 def test_pure_helpers():
     lib = _native.load()
-    assert lib.sbfs_abi_version() == 1
+    assert lib.sbfs_abi_version() == 2
     assert lib.sbfs_word_stride(12) == 2      # 121 bits
     assert lib.sbfs_word_stride(28) == 12     # 729 bits
     assert lib.sbfs_word_stride(2) == 1
@@ -87,3 +87,5 @@ def test_noalloc_entry_rejects_bad_sizes_before_touching_a_device():
     assert lib.sbfs_solve_small_noalloc(None, 32, 8, 1, None, None, 0, ctypes.byref(fv), None) == 1
     words = (ctypes.c_uint64 * 2)()
     assert lib.sbfs_solve_small_noalloc(maps, 32, 8, 1, None, words, 0, ctypes.byref(fv), None) == 1
+    # lengths are required: a malformed record is reported only through them
+    assert lib.sbfs_solve_small_noalloc(maps, 32, 8, 1, None, words, 2, ctypes.byref(fv), None) == 1

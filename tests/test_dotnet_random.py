@@ -112,3 +112,22 @@ def test_oracle_on_integrity_batch(oracle_mod):
     sync = ref["len"] >= 0
     assert 0.5 < sync.mean() < 1.0   # random binary automata mostly synchronise
     assert oracle_mod.replay(recs, ref["len"], ref["words"], n=n)[0] == 0
+
+
+@pytest.mark.parametrize("seed", SEEDS)
+def test_oracle_generator_equals_restatement(seed, oracle_mod):
+    """The oracle's own System.Random (used by the CPU baseline, which must not
+    load the product library) gives the same outputs and batches."""
+    r = D.DotnetRandom(seed)
+    assert oracle_mod.dotnet_random_next(seed, 300).tolist() == [r.Next() for _ in range(300)]
+
+
+@pytest.mark.parametrize("n,lstride", [(1, 1), (8, 8), (12, 12), (13, 32), (20, 20), (28, 32)])
+def test_oracle_batch_equals_native_batch(n, lstride, oracle_mod):
+    seed = 1234567 + 5000
+    mine = oracle_mod.fill_array_of_problems(5000, n, seed, lstride, threads=3)
+    np.testing.assert_array_equal(mine, D.fill_array_of_problems(5000, n, seed, lstride=lstride))
+    probs = D.fill_array_of_problems_py(50, n, seed)
+    for i, p in enumerate(probs):
+        assert mine[i, :n].tolist() == p.stateTransitioningMatrixA
+        assert mine[i, lstride:lstride + n].tolist() == p.stateTransitioningMatrixB

@@ -438,3 +438,60 @@ def test_permutation_automata_on_every_class(engine, oracle_mod):
     r = engine.solve(recs, ns=ns)
     assert (r["len"] == -1).all()
     np.testing.assert_array_equal(r["len"], oracle_mod.solve(recs, ns=ns, words=False)["len"])
+
+
+def test_bounded_device_wait_runs_out_and_the_handle_recovers(oracle_mod):
+    """The streamed host path's kernel waits, bounded, for each chunk of records
+    to arrive.  Withhold one chunk's ready flag (a host-side hook: the records
+    still arrive, the flag does not) with a short poll limit: the wait runs out,
+    the call returns SBFS_ETIMEOUT, and the same handle then solves the next
+    batch exactly."""
+    import os
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    count, n = 1 << 19, 12                     # four 2^17 chunks: the streamed path
+    recs = P.repack(P.uniform_maps(count, n, 0xB0B), 32, n)
+    os.environ["SBFS_TEST_SKIP_CHUNK_READY"] = "2"
+    try:
+        eng = sbfs.Engine(device=0, wait_polls=1 << 10)
+    finally:
+        del os.environ["SBFS_TEST_SKIP_CHUNK_READY"]
+    with eng:
+        with pytest.raises(sbfs.SbfsError) as ei:
+            eng.solve(recs, n=n, lstride=n)
+        assert ei.value.status == 3            # SBFS_ETIMEOUT
+        r = eng.solve(recs, n=n, lstride=n)
+    ref = oracle_mod.solve(recs, n=n, lstride=n, words=False, threads=8)
+    np.testing.assert_array_equal(r["len"], ref["len"])
+    assert oracle_mod.replay(recs, r["len"], r["words"], n=n, lstride=n)[0] == 0
+
+
+def test_config3_mixed_full_batch_as_benchmarked(engine, oracle_mod):
+    """The mixed configuration exactly as bench.py times it: 200,000 automata,
+    n uniform in 6..20, 1 % Cerny family (expected length (n-1)^2); every
+    length against the oracle, every word replayed."""
+    import bench
+    wl = bench.make_workload("mixed")
+    assert wl["count"] == 200_000
+    r = engine.solve(wl["recs"], ns=wl["ns"], lstride=32)
+    ref = _check(oracle_mod, wl["recs"], r, ns=wl["ns"])
+    cerny = np.arange(0, wl["count"], 100)
+    np.testing.assert_array_equal(r["len"][cerny], (wl["ns"][cerny].astype(np.int32) - 1) ** 2)
+    assert ref["len"].max() == 19 * 19
+
+
+def test_config5_large_instances_as_named(engine, oracle_mod):
+    """The large configuration exactly as named: n = 24, 26, 28, each with 64
+    uniform random automata, the Cerny automaton C_n and a random permutation
+    plus one merge; every length against the oracle (which runs the same
+    power-set BFS on the host), every word replayed."""
+    import bench
+    wl = bench.make_workload("large")
+    assert wl["count"] == 3 * 66
+    r = engine.solve(wl["recs"], ns=wl["ns"], lstride=32)
+    ref = _check(oracle_mod, wl["recs"], r, ns=wl["ns"])
+    for n in (24, 26, 28):
+        idx = np.nonzero(wl["ns"] == n)[0]
+        assert r["len"][idx[64]] == (n - 1) ** 2              # C_n
+    assert (ref["len"] >= 0).sum() > 100

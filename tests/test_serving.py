@@ -4,8 +4,12 @@
 * a request gives the same length alone and in the mix (words may differ:
   shortest words are not unique, each must replay);
 * malformed requests are refused at submission, a full queue refuses with
-  SBFS_EBUSY, cancelling a pending request returns SBFS_ECANCELED.
+  SBFS_EBUSY, cancelling a pending request returns SBFS_ECANCELED;
+* a mini-batch whose work failed completes its requests with SBFS_ECUDA, never
+  with stale results, and so does every later request (the failure is made on
+  the host: SBFS_SERVER_FAIL_BATCH reports one batch's event as failed).
 """
+import os
 import time
 
 import numpy as np
@@ -34,7 +38,7 @@ def _skip_without_gpu():
 
 def test_serving_matches_oracle(oracle_mod):
     _skip_without_gpu()
-    recs, ns = _requests(1500, 31)
+    recs, ns = _requests(1500, 31, hi=24)   # the serving workload's sizes: up to n = 24
     with Server(device=0) as srv:
         ids = [srv.submit_record(recs[i], int(ns[i])) for i in range(len(ns))]
         res = srv.wait_all(ids)
@@ -94,3 +98,26 @@ def test_admission_and_cancellation():
         assert all(r["len"] == 21 * 21 for r in done)
         assert sum(r["status"] == 7 for r in res.values()) == cancelled
         assert srv.stats()["arena_peak"] <= fp
+
+
+def test_failed_batch_completes_with_an_error_not_stale_results(oracle_mod):
+    _skip_without_gpu()
+    recs, ns = _requests(600, 57, lo=4, hi=16, cerny_every=50)
+    os.environ["SBFS_SERVER_FAIL_BATCH"] = "2"
+    try:
+        srv = Server(device=0, max_batch=64)
+    finally:
+        del os.environ["SBFS_SERVER_FAIL_BATCH"]
+    with srv:
+        ids = [srv.submit_record(recs[i], int(ns[i])) for i in range(len(ns))]
+        res = srv.wait_all(ids, timeout_s=120)
+        late = [srv.submit_record(recs[i], int(ns[i])) for i in range(5)]
+        late_res = srv.wait_all(late, timeout_s=60)
+    status = np.array([res[i]["status"] for i in ids])
+    assert set(status.tolist()) <= {0, 4} and (status == 4).sum() > 0
+    ok = np.nonzero(status == 0)[0]
+    ref = oracle_mod.solve(recs, ns=ns, words=False, threads=8)
+    got = np.array([res[ids[i]]["len"] for i in ok], dtype=np.int32)
+    np.testing.assert_array_equal(got, ref["len"][ok])
+    assert all(res[ids[i]]["len"] == -1 for i in np.nonzero(status == 4)[0])
+    assert all(r["status"] == 4 for r in late_res.values())
