@@ -74,7 +74,7 @@ def parse_args(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["sbfs", "reference"], default="sbfs")
     ap.add_argument("--workload", choices=["n12", "n8", "n13", "mixed", "large", "serving"], default="n12")
-    ap.add_argument("--rates", default="2000,8000,32000,128000,0",
+    ap.add_argument("--rates", default="2000,8000,32000,128000,512000,0",
                     help="serving: offered request rates per second (0 = submit all at once)")
     ap.add_argument("--count", type=int, default=0, help="automata per GPU (0 = the workload's size)")
     ap.add_argument("--max-batch", type=int, default=0, help="serving: small requests per mini-batch (0 = 8192)")
@@ -85,6 +85,8 @@ def parse_args(argv=None):
     ap.add_argument("--plain-sample", type=int, default=2000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="n12: skip the serving-latency summary")
+    ap.add_argument("--serving-requests", type=int, default=100_000,
+                    help="n12: requests of each rate of the serving-latency summary")
     ap.add_argument("--no-extra", action="store_true", help="n12: skip the mixed / large / n13 summaries")
     ap.add_argument("--extra-steps", type=int, default=5, help="timed steps of each extra summary")
     ap.add_argument("--no-tune", action="store_true", help="keep the default kernel shapes")
@@ -566,9 +568,12 @@ def run_sbfs(args):
                     return {"offered_per_s": e["offered_per_s"], "achieved_per_s": e["achieved_automata_per_s"],
                             "p50_ms_n_le_20": e["latency_ms_n_le_20"]["p50"],
                             "p99_ms_n_le_20": e["latency_ms_n_le_20"]["p99"],
-                            "p99_ms_all": e["latency_ms"]["p99"]}
-                line["serving"] = {"requests": 10_000,
-                                   "sweep": [brief(e) for e in serve_sweep(10_000, [32000.0, 0.0])],
+                            "p99_ms_all": e["latency_ms"]["p99"], "client_lag_ms_p99": e["client_lag_ms_p99"],
+                            "peak_hbm_admitted_bytes": e["peak_arena_bytes"] + e["peak_small_footprint_bytes"],
+                            "statuses_ok": e["statuses_ok"]}
+                line["serving"] = {"requests": args.serving_requests,
+                                   "sweep": [brief(e) for e in serve_sweep(args.serving_requests,
+                                                                           [32000.0, 256000.0, 0.0])],
                                    "full_sweep": "bench.py --workload serving"}
             if not args.no_extra:
                 line.update(extra_summaries(args, eng, dev, stream, flush, hbm_peak, threads))
@@ -659,7 +664,10 @@ def extra_summaries(args, eng, dev, stream, flush, hbm_peak: float, threads: int
 def serve_sweep(count, rates, max_batch=0, max_levels=0):
     """Open-loop Poisson sweep of single-automaton requests through the serving
     loop (n log-uniform 8..24, 5 % Cerny family); one entry per offered rate
-    (0 = all submitted at once)."""
+    (0 = all submitted at once).  A client thread submits, at every moment,
+    all requests whose arrival time has passed in one sbfs_server_submit_many
+    call; a request's latency is its time in the server (submission to
+    result) plus how late the client submitted it after its arrival."""
     import threading
 
     import numpy as np
@@ -673,62 +681,75 @@ def serve_sweep(count, rates, max_batch=0, max_levels=0):
     cerny = np.arange(0, count, 20)          # 5% Cerny family
     for i in cerny:
         recs[i] = P.cerny_record(int(ns[i]))
-    a_rows = [np.ascontiguousarray(recs[i, :ns[i]]) for i in range(count)]
-    b_rows = [np.ascontiguousarray(recs[i, 32:32 + ns[i]]) for i in range(count)]
     rng = np.random.default_rng(seed)
     sweep = []
-    srv = Server(device=0, max_batch=max_batch, max_levels=max_levels)
+    srv = Server(device=0, max_batch=max_batch, max_levels=max_levels, queue_capacity=max(1 << 20, 2 * count))
+
+    def collect(want, t_limit):
+        got = []
+        have = 0
+        while have < want:
+            a = srv.poll_array(timeout_ms=20)
+            if a.size:
+                got.append(a)
+                have += a.size
+            elif time.perf_counter() > t_limit:
+                raise SystemExit("serving run did not finish")
+        return np.concatenate(got) if got else np.zeros(0)
+
     # warm-up: the whole request set once, so every kernel the sweep uses has been
     # loaded and launched before anything is timed
-    warm = [srv.submit(a_rows[i], b_rows[i], int(ns[i])) for i in range(count)]
-    srv.wait_all(warm)
+    srv.submit_many(recs, ns)
+    collect(count, time.perf_counter() + 600)
     for rate in rates:
         srv.reset_peak()
         gaps = rng.exponential(1.0 / rate, count) if rate > 0 else np.zeros(count)
-        times = np.cumsum(gaps)
-        ids = [0] * count
-        refused = [0]
+        arrive = np.cumsum(gaps)
+        ids = np.zeros(count, dtype=np.uint64)
+        lag = np.zeros(count)
+        retries = [0]
 
         def submitter():
             t0 = time.perf_counter()
-            for i in range(count):
-                target = t0 + times[i]
-                while True:
-                    now = time.perf_counter()
-                    if now >= target:
-                        break
-                    if target - now > 2e-4:
-                        time.sleep((target - now) * 0.5)
-                while True:
-                    try:
-                        ids[i] = srv.submit(a_rows[i], b_rows[i], int(ns[i]))
-                        break
-                    except Exception:
-                        refused[0] += 1
-                        time.sleep(1e-4)
+            i = 0
+            while i < count:
+                now = time.perf_counter() - t0
+                j = int(np.searchsorted(arrive, now, side="right"))
+                if j <= i:
+                    wait = arrive[i] - now
+                    if wait > 2e-4:
+                        time.sleep(wait * 0.5)
+                    continue
+                try:
+                    ids[i:j] = srv.submit_many(recs[i:j], ns[i:j])
+                except Exception:
+                    retries[0] += 1
+                    time.sleep(1e-4)
+                    continue
+                lag[i:j] = (time.perf_counter() - t0) - arrive[i:j]
+                i = j
 
         th = threading.Thread(target=submitter)
         t_start = time.perf_counter()
         th.start()
-        results = {}
-        while len(results) < count:
-            for r in srv.poll(timeout_ms=20):
-                results[r["id"]] = r
-            if not th.is_alive() and len(results) < count and time.perf_counter() - t_start > 600:
-                raise SystemExit("serving run did not finish")
+        res = collect(count, t_start + 600)
         th.join()
         wall = time.perf_counter() - t_start
         st = srv.stats()
-        by_id = [results[i] for i in ids]
-        lat = np.array([r["done_ms"] - r["submit_ms"] for r in by_id])
-        small = np.array([int(r["n"]) <= 20 for r in by_id])
-        tiny = np.array([int(r["n"]) <= 16 for r in by_id])
+        order = np.argsort(res["id"])
+        res = res[order]
+        pos = np.searchsorted(res["id"], ids)
+        res = res[pos]                      # in submission order
+        lat = (res["done_ms"] - res["submit_ms"]) + lag * 1e3
+        n_of = res["n"]
+        small = n_of <= 20
+        tiny = n_of <= 16
         mid = small & ~tiny
-        first = min(r["submit_ms"] for r in by_id)
-        last = max(r["done_ms"] for r in by_id)
+        span_ms = float(res["done_ms"].max() - res["submit_ms"].min())
         entry = {
             "offered_per_s": rate if rate > 0 else "all at once",
-            "achieved_automata_per_s": count / ((last - first) / 1e3),
+            "requests": count,
+            "achieved_automata_per_s": count / (span_ms / 1e3),
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                            "max": float(lat.max())},
             "latency_ms_n_le_20": {"p50": float(np.percentile(lat[small], 50)),
@@ -737,7 +758,10 @@ def serve_sweep(count, rates, max_batch=0, max_levels=0):
                                    "p99": float(np.percentile(lat[tiny], 99))},
             "latency_ms_n_17_20": {"p50": float(np.percentile(lat[mid], 50)),
                                    "p99": float(np.percentile(lat[mid], 99))},
-            "peak_arena_bytes": int(st["arena_peak"]), "submit_retries": refused[0], "wall_s": wall,
+            "client_lag_ms_p99": float(np.percentile(lag, 99) * 1e3),
+            "peak_arena_bytes": int(st["arena_peak"]), "peak_small_footprint_bytes": int(st["small_peak"]),
+            "statuses_ok": bool((res["status"] == 0).all()),
+            "submit_retries": retries[0], "wall_s": wall,
         }
         sweep.append(entry)
         print(json.dumps({"serving_rate": entry}), file=sys.stderr, flush=True)
@@ -748,7 +772,7 @@ def serve_sweep(count, rates, max_batch=0, max_levels=0):
 def run_serving(args):
     if int(os.environ.get("RANK", "0")) != 0:
         return 0
-    count = args.count or 20_000
+    count = args.count or 100_000
     rates = [float(r) for r in args.rates.split(",")]
     sweep = serve_sweep(count, rates, args.max_batch, args.max_levels)
     best = max(sweep, key=lambda e: e["achieved_automata_per_s"])

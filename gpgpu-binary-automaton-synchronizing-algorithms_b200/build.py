@@ -19,6 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIBDIR = os.path.join(HERE, "sbfs", "_lib")
 LIB = os.path.join(LIBDIR, "libsbfs.so")
+CHECKED_LIB = os.path.join(LIBDIR, "libsbfs_checked.so")
 INCLUDE = os.path.join(ROOT, "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -45,8 +46,14 @@ def _compile(src: str, obj: str, extra):
     return r.stderr
 
 
-def build(force: bool = False, verbose: bool = False, extra=()) -> str:
-    os.makedirs(BUILD, exist_ok=True)
+def build(force: bool = False, verbose: bool = False, extra=(), checked: bool = False) -> str:
+    """Compiles the library; checked=True builds libsbfs_checked.so instead, with
+    -DSBFS_CHECKED (data-derived indices checked on the device, failures
+    reported as an error status; see csrc/common.cuh)."""
+    build_dir = os.path.join(BUILD, "checked") if checked else BUILD
+    lib = CHECKED_LIB if checked else LIB
+    extra = list(extra) + (["-DSBFS_CHECKED"] if checked else [])
+    os.makedirs(build_dir, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
     srcs = sorted(f for f in os.listdir(CSRC) if f.endswith(".cu"))
     newest_header = max((os.path.getmtime(h) for h in _headers()), default=0)
@@ -54,7 +61,7 @@ def build(force: bool = False, verbose: bool = False, extra=()) -> str:
     objs = []
     for f in srcs:
         src = os.path.join(CSRC, f)
-        obj = os.path.join(BUILD, f[:-3] + ".o")
+        obj = os.path.join(build_dir, f[:-3] + ".o")
         objs.append(obj)
         stale = force or not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(src),
                                                                                  newest_header)
@@ -67,16 +74,16 @@ def build(force: bool = False, verbose: bool = False, extra=()) -> str:
                 msg = fu.result()
                 if verbose and msg:
                     print(msg, file=sys.stderr)
-    if jobs or not os.path.exists(LIB) or force:
-        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+    if jobs or not os.path.exists(lib) or force:
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", lib] + objs + ["-lcudart"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":
     force = "--force" in sys.argv
     verbose = "-v" in sys.argv
     extra = ["-Xptxas", "-v"] if "--ptxas" in sys.argv else []
-    print(build(force=force, verbose=verbose or bool(extra), extra=extra))
+    print(build(force=force, verbose=verbose or bool(extra), extra=extra, checked="--checked" in sys.argv))

@@ -876,7 +876,8 @@ sbfs_status solve_host(sbfs_handle *h, const uint8_t *maps, int32_t lstride, con
                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         }
         if (so.error & kErrInvalid) return fail(h, SBFS_EINVAL, "malformed automaton: a state index >= n");
-        if (so.error) return fail(h, SBFS_ETIMEOUT, "a device-side bounded wait ran out");
+        if (so.error & kErrBounds) return fail(h, SBFS_ECUDA, "a bounds check failed (checked build)");
+    if (so.error) return fail(h, SBFS_ETIMEOUT, "a device-side bounded wait ran out");
         return SBFS_OK;
     }
     const int64_t chunk = plain ? std::max<int64_t>(count, 1)
@@ -1033,6 +1034,7 @@ sbfs_status solve_host(sbfs_handle *h, const uint8_t *maps, int32_t lstride, con
             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
     if (tot.error & kErrInvalid) return fail(h, SBFS_EINVAL, "malformed automaton: a state index >= n");
+    if (tot.error & kErrBounds) return fail(h, SBFS_ECUDA, "a bounds check failed (checked build)");
     if (tot.error) return fail(h, SBFS_ETIMEOUT, "a device-side bounded wait ran out");
     return SBFS_OK;
 }
@@ -1334,6 +1336,7 @@ sbfs_status sbfs_device_wait(sbfs_handle *h, sbfs_stats *stats)
         cudaGetLastError();
     }
     if (c->error & kErrInvalid) return fail(h, SBFS_EINVAL, "malformed automaton: a state index >= n");
+    if (c->error & kErrBounds) return fail(h, SBFS_ECUDA, "a bounds check failed (checked build)");
     if (c->error) return fail(h, SBFS_ETIMEOUT, "a device-side bounded wait ran out");
     return SBFS_OK;
 }

@@ -18,6 +18,18 @@ constexpr int32_t kLenInvalid = -2;   // malformed record (state >= n); host tur
 constexpr int kErrInvalid = 1;        // malformed automaton seen
 constexpr int kErrCapacity = 2;       // a queue or frontier exceeded its reserved space
 constexpr int kErrWait = 4;           // a bounded wait for streamed input ran out
+constexpr int kErrBounds = 8;         // a checked build's index check failed (the access was skipped)
+
+// Checked builds (-DSBFS_CHECKED, libsbfs_checked.so): an index that comes
+// from data (an image, a queue position, a list slot) is checked before the
+// access; a failed check records kErrBounds in the launch's error word, which
+// the host reports as SBFS_ECUDA, and the access is skipped -- no fault, no
+// trap.  In the regular build the check compiles to nothing.
+#ifdef SBFS_CHECKED
+#define SBFS_CHECK(cond, err) ((cond) || (atomicOr((err), kErrBounds), false))
+#else
+#define SBFS_CHECK(cond, err) true
+#endif
 
 // Everything a BFS kernel needs to know about the batch.
 struct Batch {

@@ -127,14 +127,16 @@ __global__ void __launch_bounds__(1024) k_cta(Batch b, int nb_max, uint64_t *que
                     y0 = (uint32_t)(t >> 32);
                     y1 = (uint32_t)t;
                     const uint32_t m0 = 1u << (y0 & 31u);
-                    if (!(atomicOr(&bitmap[y0 >> 5], m0) & m0)) {
+                    const bool in0 = SBFS_CHECK((y0 >> nb_max) == 0u, b.error);
+                    const bool in1 = SBFS_CHECK((y1 >> nb_max) == 0u, b.error);
+                    if (in0 && !(atomicOr(&bitmap[y0 >> 5], m0) & m0)) {
                         if (is_singleton(y0))
                             atomicMin(found, ((unsigned long long)i << 1));
                         else
                             p0 = true;
                     }
                     const uint32_t m1 = 1u << (y1 & 31u);
-                    if (!(atomicOr(&bitmap[y1 >> 5], m1) & m1)) {
+                    if (in1 && !(atomicOr(&bitmap[y1 >> 5], m1) & m1)) {
                         if (is_singleton(y1))
                             atomicMin(found, ((unsigned long long)i << 1) | 1ull);
                         else
@@ -150,8 +152,11 @@ __global__ void __launch_bounds__(1024) k_cta(Batch b, int nb_max, uint64_t *que
                     pos = __shfl_sync(kFull, pos, 0);
                     const unsigned lt = (1u << lane) - 1u;
                     pos += __popc(m0 & lt) + __popc(m1 & lt);
-                    if (p0) queue[pos++] = y0 | ((uint64_t)i << 32);
-                    if (p1) queue[pos] = y1 | ((uint64_t)i << 32) | (1ull << 63);
+                    // every subset enters the queue at most once: 2^nb_max entries never overflow
+                    if (p0 && SBFS_CHECK(pos < (1u << nb_max), b.error)) queue[pos] = y0 | ((uint64_t)i << 32);
+                    pos += p0 ? 1u : 0u;
+                    if (p1 && SBFS_CHECK(pos < (1u << nb_max), b.error))
+                        queue[pos] = y1 | ((uint64_t)i << 32) | (1ull << 63);
                 }
             }
             __syncthreads();

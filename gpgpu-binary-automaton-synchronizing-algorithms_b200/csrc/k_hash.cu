@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(HashGeom<CAP_BITS>::kWarps * 32)
             }
             const int sa_slot = has ? set_insert<CAP_BITS>(W.set, ya, gen) : -1;
             const int sb_slot = has ? set_insert<CAP_BITS>(W.set, yb, gen) : -1;
-            const bool fa = sa_slot >= 0, fb = sb_slot >= 0;
+            bool fa = sa_slot >= 0, fb = sb_slot >= 0;
             const unsigned ma = __ballot_sync(kFull, fa), mb = __ballot_sync(kFull, fb);
             const uint32_t added = (uint32_t)(__popc(ma) + __popc(mb));
             if (tail + added > kHashLimit) {
@@ -183,6 +183,7 @@ __global__ void __launch_bounds__(HashGeom<CAP_BITS>::kWarps * 32)
             }
             const unsigned lt = (1u << lane) - 1u;
             uint32_t p = tail + (uint32_t)(__popc(ma & lt) + __popc(mb & lt));
+            if (!SBFS_CHECK(p + (fa ? 1u : 0u) + (fb ? 1u : 0u) <= kHashLimit, b.error)) fa = fb = false;
             if (fa) {
                 W.queue[p] = (uint16_t)sa_slot;
                 W.parent[p++] = (uint16_t)idx;

@@ -78,6 +78,7 @@ __global__ void __launch_bounds__(512) k_pool(Batch b, int q_smem, int grab, uin
                                : __ldcg(spill_warp + (size_t)s * spill_per_slot + (i - (uint32_t)Q));
     };
     auto qstore = [&](int s, uint32_t i, uint32_t v) {
+        if (!SBFS_CHECK(i < (uint32_t)Q + spill_per_slot, b.error)) return;
         if (i < (uint32_t)Q)
             queue[s * Q + i] = v;
         else
@@ -212,13 +213,14 @@ __global__ void __launch_bounds__(512) k_pool(Batch b, int q_smem, int grab, uin
             img0 = t >> 16;
             img1 = t & 0xFFFFu;
             uint32_t *bm = bitmap + s_item * BW;
+            const bool in = SBFS_CHECK((img0 >> 5) < (uint32_t)BW && (img1 >> 5) < (uint32_t)BW, b.error);
             const uint32_t bit0 = 1u << (img0 & 31u);
-            if (!(atomicOr(&bm[img0 >> 5], bit0) & bit0)) {
+            if (in && !(atomicOr(&bm[img0 >> 5], bit0) & bit0)) {
                 push0 = true;
                 fnd0 = is_singleton(img0);
             }
             const uint32_t bit1 = 1u << (img1 & 31u);
-            if (!(atomicOr(&bm[img1 >> 5], bit1) & bit1)) {
+            if (in && !(atomicOr(&bm[img1 >> 5], bit1) & bit1)) {
                 push1 = true;
                 fnd1 = is_singleton(img1);
             }

@@ -66,6 +66,7 @@ struct SmallSlot {
     size_t left = 0;                     // requests not yet delivered
     unsigned int tag = 0;                // this launch's flag value
     int64_t seq = 0;                     // 1-based launch number of the mini-batch
+    int64_t footprint = 0;               // admitted bytes: 2^n / 8 + 64 per request
     cudaEvent_t ev = nullptr;
     bool busy = false;
 };
@@ -92,6 +93,7 @@ struct sbfs_server {
     SmallSlot small[kSmallSlots];
     unsigned int next_tag = 1;
     Arena arena;                                   // HBM budget of the admitted large requests
+    int64_t small_used = 0, small_peak = 0;        // footprint of the mini-batches in flight
     LevelEngine big;                               // level slots for n >= 21
     std::unordered_map<long long, Request> large;   // admitted, keyed by id
     std::string error;
@@ -135,12 +137,26 @@ enum class Ev { kPending, kDone, kFailed };
 Ev event_state(cudaEvent_t ev, cudaError_t *err);
 void fail_all(sbfs_server *s, int32_t status, const std::string &why);
 
+// Bytes an n <= 20 request accounts for while its mini-batch is in flight: its
+// 2^n-bit visited set (the store the batch kernels keep on chip, or in HBM for
+// a hand-off) and its 64-byte record.
+int64_t small_footprint(int n)
+{
+    return (int64_t)(((uint64_t)1 << n) / 8) + 64;
+}
+
 bool launch_small(sbfs_server *s, SmallSlot &S)
 {
     Lane &L = s->h->lanes[(size_t)S.lane];
     const int cap = s->cfg.max_batch;
     S.reqs.clear();
+    // admission by footprint: a request accounts for its 2^n-bit visited set
+    // and its record; the mini-batches in flight stay within small_budget_bytes
+    int64_t fp = 0;
     while (!s->pend_small.empty() && (int)S.reqs.size() < cap) {
+        const int64_t need = small_footprint(s->pend_small.front().n);
+        if (s->small_used + fp + need > s->cfg.small_budget_bytes && (fp > 0 || s->small_used > 0)) break;
+        fp += need;
         S.reqs.push_back(s->pend_small.front());
         s->pend_small.pop_front();
     }
@@ -180,6 +196,7 @@ bool launch_small(sbfs_server *s, SmallSlot &S)
         S.delivered.assign((size_t)cnt, 0);
         S.left = (size_t)cnt;
         S.busy = true;   // fail_all completes this slot's requests
+        S.footprint = 0;
         fail_all(s, SBFS_ECUDA, std::string("serving: ") + cudaGetErrorString(ce));
         return true;
     }
@@ -187,6 +204,9 @@ bool launch_small(sbfs_server *s, SmallSlot &S)
     S.left = (size_t)cnt;
     S.busy = true;
     S.seq = ++s->batches_launched;
+    S.footprint = fp;
+    s->small_used += fp;
+    s->small_peak = std::max(s->small_peak, s->small_used);
     std::lock_guard<std::mutex> lock(s->mu);
     s->st.small_batches++;
     return true;
@@ -234,6 +254,8 @@ bool poll_small(sbfs_server *s, SmallSlot &S)
     if (finished) {
         S.reqs.clear();
         S.busy = false;
+        s->small_used -= S.footprint;
+        S.footprint = 0;
         progress = true;
     }
     return progress;
@@ -308,6 +330,8 @@ void fail_all(sbfs_server *s, int32_t status, const std::string &why)
         S.reqs.clear();
         S.left = 0;
         S.busy = false;
+        s->small_used -= S.footprint;
+        S.footprint = 0;
     }
     for (auto &kv : s->large) complete(s, kv.second, status, -1, nullptr);
     s->large.clear();
@@ -393,6 +417,7 @@ void run_loop(sbfs_server *s)
             std::lock_guard<std::mutex> lock(s->mu);
             if (s->reset_peak) {
                 s->arena.reset_peak();
+                s->small_peak = s->small_used;
                 s->reset_peak = false;
             }
             s->st.pending = (int64_t)(s->incoming.size() + s->pend_small.size() + s->pend_big.size());
@@ -402,6 +427,9 @@ void run_loop(sbfs_server *s)
             s->st.arena_used = (int64_t)s->arena.used();
             s->st.arena_peak = (int64_t)s->arena.peak();
             s->st.arena_capacity = (int64_t)s->arena.capacity();
+            s->st.small_used = s->small_used;
+            s->st.small_peak = s->small_peak;
+            s->st.small_capacity = s->cfg.small_budget_bytes;
         }
         if (!progress) std::this_thread::sleep_for(std::chrono::microseconds(20));
     }
@@ -439,6 +467,7 @@ sbfs_status sbfs_server_start(const sbfs_server_config *cfg, sbfs_server **out)
     if (s->cfg.max_levels <= 0) s->cfg.max_levels = 16;
     if (s->cfg.queue_capacity <= 0) s->cfg.queue_capacity = 1 << 20;
     if (s->cfg.arena_bytes <= 0) s->cfg.arena_bytes = (int64_t)16 << 30;
+    if (s->cfg.small_budget_bytes <= 0) s->cfg.small_budget_bytes = (int64_t)1 << 30;
     if (const char *inj = std::getenv("SBFS_SERVER_FAIL_BATCH")) s->inject_fail_batch = std::atoll(inj);
     sbfs_config hc;
     sbfs_config_default(&hc);
@@ -514,6 +543,46 @@ sbfs_status sbfs_server_submit(sbfs_server *s, const uint8_t *a, const uint8_t *
     }
     s->cv_in.notify_one();
     if (out_id) *out_id = r.id;
+    return SBFS_OK;
+}
+
+sbfs_status sbfs_server_submit_many(sbfs_server *s, const uint8_t *maps, int32_t lstride, const uint8_t *ns,
+                                    int64_t count, uint64_t *out_ids)
+{
+    if (!s || count < 0 || lstride < 1 || lstride > 32 || (count > 0 && (!maps || !ns || !out_ids)))
+        return SBFS_EINVAL;
+    for (int64_t i = 0; i < count; ++i) {
+        const uint8_t *rec = maps + (size_t)i * 2 * (size_t)lstride;
+        if (ns[i] > lstride || !valid(rec, rec + lstride, ns[i])) {
+            std::lock_guard<std::mutex> lock(s->mu);
+            s->st.rejected += count;
+            return SBFS_EINVAL;
+        }
+    }
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        if (s->stopping) return SBFS_ESTOPPED;
+        if (s->st.pending + count > s->cfg.queue_capacity ||
+            (int64_t)s->incoming.size() + count > s->cfg.queue_capacity) {
+            s->st.rejected += count;
+            return SBFS_EBUSY;
+        }
+        const double now = s->now_ms();
+        for (int64_t i = 0; i < count; ++i) {
+            const uint8_t *rec = maps + (size_t)i * 2 * (size_t)lstride;
+            Request r;
+            std::memset(&r, 0, sizeof(r));
+            r.n = ns[i];
+            std::memcpy(r.a, rec, (size_t)r.n);
+            std::memcpy(r.b, rec + lstride, (size_t)r.n);
+            r.id = s->next_id++;
+            r.submit_ms = now;
+            s->incoming.push_back(r);
+            out_ids[i] = r.id;
+        }
+        s->st.submitted += count;
+    }
+    s->cv_in.notify_one();
     return SBFS_OK;
 }
 

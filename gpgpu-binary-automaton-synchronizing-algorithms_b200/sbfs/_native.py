@@ -21,7 +21,8 @@ EXPORTS = [
     "sbfs_status_string", "sbfs_best_parallelism", "sbfs_solve_batch", "sbfs_verify_batch",
     "sbfs_solve_plain", "sbfs_solve_batch_device", "sbfs_device_wait", "sbfs_host_alloc",
     "sbfs_host_free", "sbfs_word_stride", "sbfs_describe_plan", "sbfs_solve_small_noalloc",
-    "sbfs_server_config_default", "sbfs_server_start", "sbfs_server_submit", "sbfs_server_poll",
+    "sbfs_server_config_default", "sbfs_server_start", "sbfs_server_submit", "sbfs_server_submit_many",
+    "sbfs_server_poll",
     "sbfs_server_cancel", "sbfs_server_stats_get", "sbfs_server_reset_peak", "sbfs_server_stop",
     "sbfs_generate_reference_batch", "sbfs_dotnet_random_next",
 ]
@@ -88,6 +89,7 @@ class ServerConfig(ctypes.Structure):
         ("max_levels", ctypes.c_int32),
         ("queue_capacity", ctypes.c_int32),
         ("arena_bytes", ctypes.c_int64),
+        ("small_budget_bytes", ctypes.c_int64),
     ]
 
 
@@ -107,7 +109,8 @@ class Result(ctypes.Structure):
 class ServerStats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_int64) for k in (
         "submitted", "completed", "rejected", "cancelled", "pending", "in_flight", "small_batches",
-        "level_launches", "arena_used", "arena_peak", "arena_capacity")] + [("now_ms", ctypes.c_double)]
+        "level_launches", "arena_used", "arena_peak", "arena_capacity")] + [("now_ms", ctypes.c_double)] + [
+        (k, ctypes.c_int64) for k in ("small_used", "small_peak", "small_capacity")]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -164,6 +167,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.sbfs_server_start.restype = ctypes.c_int
     L.sbfs_server_submit.argtypes = [P, P, P, i32, ctypes.POINTER(ctypes.c_uint64)]
     L.sbfs_server_submit.restype = ctypes.c_int
+    L.sbfs_server_submit_many.argtypes = [P, P, i32, P, i64, P]
+    L.sbfs_server_submit_many.restype = ctypes.c_int
     L.sbfs_server_poll.argtypes = [P, ctypes.POINTER(Result), i32, ctypes.POINTER(i32), i32]
     L.sbfs_server_poll.restype = ctypes.c_int
     L.sbfs_server_cancel.argtypes = [P, ctypes.c_uint64]

@@ -16,9 +16,14 @@ import numpy as np
 from . import _native
 
 
+RESULT_DTYPE = np.dtype([("id", np.uint64), ("status", np.int32), ("len", np.int32), ("n", np.int32),
+                         ("pad", np.int32), ("word", np.uint64, (12,)), ("submit_ms", np.float64),
+                         ("done_ms", np.float64)])
+
+
 class Server:
     def __init__(self, device: int = -1, max_batch: int = 0, max_levels: int = 0, queue_capacity: int = 0,
-                 arena_bytes: int = 0):
+                 arena_bytes: int = 0, small_budget_bytes: int = 0):
         self.lib = _native.load()
         cfg = _native.ServerConfig()
         self.lib.sbfs_server_config_default(ctypes.byref(cfg))
@@ -27,6 +32,7 @@ class Server:
         cfg.max_levels = max_levels
         cfg.queue_capacity = queue_capacity
         cfg.arena_bytes = arena_bytes
+        cfg.small_budget_bytes = small_budget_bytes
         h = ctypes.c_void_p()
         st = self.lib.sbfs_server_start(ctypes.byref(cfg), ctypes.byref(h))
         if st != 0:
@@ -48,6 +54,22 @@ class Server:
     def submit_record(self, rec, n: int, lstride: int = 32) -> int:
         return self.submit(rec[:n], rec[lstride:lstride + n], n)
 
+    def submit_many(self, recs, ns, lstride: int = 32) -> np.ndarray:
+        """Submits every record in one call (all admitted or none); returns
+        their ids.  Raises SbfsError (EINVAL / EBUSY)."""
+        recs = np.ascontiguousarray(recs, dtype=np.uint8)
+        ns = np.ascontiguousarray(ns, dtype=np.uint8)
+        count = int(ns.shape[0])
+        if recs.shape != (count, 2 * lstride):
+            raise ValueError(f"records must have shape ({count}, {2 * lstride})")
+        ids = np.empty(count, dtype=np.uint64)
+        st = self.lib.sbfs_server_submit_many(self.handle, recs.ctypes.data_as(ctypes.c_void_p), lstride,
+                                              ns.ctypes.data_as(ctypes.c_void_p), count,
+                                              ids.ctypes.data_as(ctypes.c_void_p))
+        if st != 0:
+            raise _native.SbfsError(st, "submit_many refused")
+        return ids
+
     def poll(self, timeout_ms: int = 0, max_results: int = 4096) -> List[dict]:
         got = ctypes.c_int32()
         self.lib.sbfs_server_poll(self.handle, self._buf, min(max_results, len(self._buf)), ctypes.byref(got),
@@ -59,6 +81,14 @@ class Server:
                         "word": np.array(r.word[:], dtype=np.uint64), "submit_ms": r.submit_ms,
                         "done_ms": r.done_ms})
         return out
+
+    def poll_array(self, timeout_ms: int = 0, max_results: int = 4096) -> np.ndarray:
+        """Like poll, as one structured array (fields of sbfs_result) -- cheap
+        for clients that collect many results."""
+        got = ctypes.c_int32()
+        self.lib.sbfs_server_poll(self.handle, self._buf, min(max_results, len(self._buf)), ctypes.byref(got),
+                                  int(timeout_ms))
+        return np.frombuffer(self._buf, dtype=RESULT_DTYPE, count=got.value).copy()
 
     def wait_all(self, ids, timeout_s: float = 120.0) -> Dict[int, dict]:
         import time

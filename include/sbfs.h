@@ -223,6 +223,9 @@ typedef struct sbfs_server_config {
     int32_t max_levels;        /* levels per launch batch of the large path; 0 = 16         */
     int32_t queue_capacity;    /* pending requests before submit returns SBFS_EBUSY; 0 = 1<<20 */
     int64_t arena_bytes;       /* HBM budget for admitted large requests; 0 = 16 GiB        */
+    int64_t small_budget_bytes; /* n <= 20: bytes the mini-batches in flight may account for,
+                                   2^n / 8 + 64 per request (its visited set and record);
+                                   0 = 1 GiB (ABI version 2)                               */
 } sbfs_server_config;
 
 typedef struct sbfs_result {
@@ -243,6 +246,7 @@ typedef struct sbfs_server_stats {
     int64_t small_batches, level_launches;
     int64_t arena_used, arena_peak, arena_capacity;  /* bytes held by admitted large requests */
     double now_ms;
+    int64_t small_used, small_peak, small_capacity;  /* footprint of the n <= 20 requests in flight */
 } sbfs_server_stats;
 
 SBFS_API sbfs_status sbfs_server_config_default(sbfs_server_config *cfg);
@@ -251,6 +255,14 @@ SBFS_API sbfs_status sbfs_server_start(const sbfs_server_config *cfg, sbfs_serve
  * malformed automaton, SBFS_EBUSY when the pending queue is full. */
 SBFS_API sbfs_status sbfs_server_submit(sbfs_server *s, const uint8_t *a, const uint8_t *b, int32_t n,
                                         uint64_t *out_id);
+/* count automata in one call, as records of 2*lstride bytes (a = rec[0..n),
+ * b = rec[lstride..lstride+n), n = ns[i]; 1 <= lstride <= 32), taken under one
+ * lock: out_ids[i] receives request i's id.  Every request is checked first;
+ * the call admits all of them or none (SBFS_EINVAL naming no request when one
+ * is malformed, SBFS_EBUSY when they do not all fit the pending queue).  For
+ * clients whose requests arrive in bursts: one call instead of count. */
+SBFS_API sbfs_status sbfs_server_submit_many(sbfs_server *s, const uint8_t *maps, int32_t lstride,
+                                             const uint8_t *ns, int64_t count, uint64_t *out_ids);
 /* Up to max finished results; waits up to timeout_ms for the first one. */
 SBFS_API sbfs_status sbfs_server_poll(sbfs_server *s, sbfs_result *out, int32_t max, int32_t *got,
                                       int32_t timeout_ms);

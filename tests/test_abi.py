@@ -67,6 +67,10 @@ def test_server_entry_points_reject_null_handles():
     rid = ctypes.c_uint64()
     a = (ctypes.c_uint8 * 3)(1, 2, 0)
     assert lib.sbfs_server_submit(None, a, a, 3, ctypes.byref(rid)) == 1
+    ids = (ctypes.c_uint64 * 1)()
+    ns = (ctypes.c_uint8 * 1)(3)
+    recs = (ctypes.c_uint8 * 64)()
+    assert lib.sbfs_server_submit_many(None, recs, 32, ns, 1, ids) == 1
     got = ctypes.c_int32()
     assert lib.sbfs_server_poll(None, None, 0, ctypes.byref(got), 0) == 1
     assert lib.sbfs_server_cancel(None, 7) == 1

@@ -121,3 +121,29 @@ def test_failed_batch_completes_with_an_error_not_stale_results(oracle_mod):
     np.testing.assert_array_equal(got, ref["len"][ok])
     assert all(res[ids[i]]["len"] == -1 for i in np.nonzero(status == 4)[0])
     assert all(r["status"] == 4 for r in late_res.values())
+
+
+def test_submit_many_and_the_small_footprint_budget(oracle_mod):
+    """Requests submitted in one call come back exactly as the oracle has them,
+    and the n <= 20 mini-batches never hold more than their footprint budget
+    (2^n / 8 + 64 bytes per request in flight)."""
+    _skip_without_gpu()
+    recs, ns = _requests(3000, 71, lo=3, hi=20, cerny_every=40)
+    budget = 4 << 20
+    with Server(device=0, small_budget_bytes=budget) as srv:
+        bad = recs[:3].copy()
+        bad[1, 0] = 63                            # state 63 in a small automaton: malformed
+        with pytest.raises(sbfs.SbfsError) as ei:
+            srv.submit_many(bad, ns[:3])
+        assert ei.value.status == 1
+        ids = srv.submit_many(recs, ns)
+        res = srv.wait_all(ids.tolist(), timeout_s=120)
+        st = srv.stats()
+    lens = np.array([res[int(i)]["len"] for i in ids], dtype=np.int32)
+    words = np.stack([res[int(i)]["word"] for i in ids])
+    ref = oracle_mod.solve(recs, ns=ns, words=False, threads=8)
+    np.testing.assert_array_equal(lens, ref["len"])
+    assert oracle_mod.replay(recs, lens, words, ns=ns)[0] == 0
+    assert 0 < st["small_peak"] <= budget and st["small_used"] == 0
+    assert st["small_batches"] > 1                # the budget split the burst into several mini-batches
+    assert st["rejected"] == 3
