@@ -15,12 +15,11 @@
 // entry carries the letters of the word that reaches it (bit NMAX + d =
 // letter d, 1 = b), so a word needs no parent pointers or retained history.
 //
-// Each iteration a lane takes up to kStep (4) subsets from its ring in queue
-// order -- across the boundary between the current level and the next, as the
-// sequential loop pops them -- and looks up their eight images: more
-// independent work per step hides the latencies that one warp's dependent
-// chain exposes at 7 warps per SM (2 -> 4 subsets: 0.64 -> 0.56 ms per 10^6
-// automata at n = 12; 6 and 8 were slower again).  A singleton among them ends the search (no singleton
+// Each iteration a lane takes up to kStep (4) subsets of its current level and
+// looks up their eight images: more independent work per step hides the
+// shared-memory latencies that one warp's dependent chain exposes at 7 warps
+// per SM (2 -> 4 subsets: 0.64 -> 0.56 ms per 10^6 automata at n = 12; 6 and 8
+// were slower again).  A singleton among them ends the search (no singleton
 // is visited before the first one is generated, so it needs no bitmap test).
 // Otherwise the eight images are test-and-set with shared-memory atomicOr, issued
 // back to back and kept in program order by the hardware for a repeated
@@ -451,100 +450,73 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
 
         // ---- up to kStep expansions per active lane ----------------------------
         if (state == kActive) {
-            // The ring holds [head, tail): the rest of the current level (up to
-            // lvl_end), then the next level's entries found so far.  A step takes
-            // up to kStep of them in queue order, across the level boundary (the
-            // sequential loop pops them in that order too); a lane with fewer
-            // left expands its first one again in the spare places, whose images
-            // are already visited by the time they are tested.
+            // a lane with fewer than kStep subsets left in the level expands its
+            // first one again in the spare places: those copies' images are
+            // already visited by the time they are tested
             constexpr int P = kStep;
-            const uint32_t take = min(tail - head, (uint32_t)P);
-            const uint32_t in_cur = min(lvl_end - head, take);   // taken entries of the current level (>= 1)
+            const uint32_t take = min(lvl_end - head, (uint32_t)P);
             uint32_t e[P];
 #pragma unroll
             for (int i = 0; i < P; ++i)
                 e[i] = (i == 0 || (uint32_t)i < take) ? rq[((head + (uint32_t)i) & rmask) * 32] : e[0];
             head += take;
             expanded += take;
-            uint32_t t[P];
-#pragma unroll
-            for (int i = 0; i < P; ++i) t[i] = lane_image<NMAX>(tb, e[i] & G::kMask);
-            // both images of a subset at once: t = a << 16 | b with a, b != 0, so
-            // t & (t - 0x10001) = (a & (a - 1)) << 16 | (b & (b - 1))
-            bool single = false;
+            uint32_t y[2 * P], hi[2 * P];
+            // entries carry the word that reaches them: the parent's letters,
+            // plus letter `level` = b for the b-images (an entry holds 32 - NMAX
+            // letters; at level >= 32 - NMAX a fresh image escalates instead)
+            const uint32_t lb = (WORDS && level < (uint32_t)G::kWordMax) ? 1u << (level + NMAX) : 0u;
 #pragma unroll
             for (int i = 0; i < P; ++i) {
-                const uint32_t q = t[i] & (t[i] - 0x10001u);
-                single |= (q < 0x10000u) | ((q & 0xFFFFu) == 0u);
+                const uint32_t t = lane_image<NMAX>(tb, e[i] & G::kMask);
+                y[2 * i] = t >> 16;
+                y[2 * i + 1] = t & 0xFFFFu;
+                hi[2 * i] = WORDS ? (e[i] & ~G::kMask) : 0u;
+                hi[2 * i + 1] = WORDS ? ((e[i] & ~G::kMask) | lb) : 0u;
             }
-            if (single) {
-                // no singleton is ever visited (the search stops at the first one),
-                // so the first singleton image in queue order (a before b) ends it
-                int sc = 2 * P;
+            // no singleton is ever visited (the search stops at the first one), so
+            // a singleton image ends the search without a bitmap test
+            int sc = -1;
 #pragma unroll
-                for (int c = 2 * P - 1; c >= 0; --c) {
-                    const uint32_t y = (c & 1) ? (t[c >> 1] & 0xFFFFu) : (t[c >> 1] >> 16);
-                    if (is_singleton(y)) sc = c;
-                }
+            for (int c = 2 * P - 1; c >= 0; --c)
+                if (is_singleton(y[c])) sc = c;
+            if (sc >= 0) {
+                state = kDone;
+                res_len = (int32_t)level + 1;
                 uint32_t es = e[0];
 #pragma unroll
                 for (int i = 1; i < P; ++i)
                     if ((sc >> 1) == i) es = e[i];
-                const uint32_t lv = level + ((uint32_t)(sc >> 1) >= in_cur ? 1u : 0u);
-                state = kDone;
-                res_len = (int32_t)lv + 1;
-                // an entry at level lv carries letters 0..lv-1 (lv <= 32 - NMAX)
-                res_word = WORDS ? ((es >> NMAX) | ((uint32_t)(sc & 1) << lv)) : 0u;
+                res_word = WORDS ? ((es >> NMAX) | ((uint32_t)(sc & 1) << level)) : 0u;
             } else {
                 // test-and-set in queue order: a subset met twice in this step is
                 // fresh only the first time (same-address atomics keep program order)
-                uint32_t y[2 * P], old[2 * P];
-#pragma unroll
-                for (int i = 0; i < P; ++i) {
-                    y[2 * i] = t[i] >> 16;
-                    y[2 * i + 1] = t[i] & 0xFFFFu;
-                }
+                uint32_t old[2 * P];
 #pragma unroll
                 for (int c = 0; c < 2 * P; ++c)
                     old[c] = SBFS_CHECK((y[c] >> 5) < (uint32_t)BW, b.error)
                                  ? atomicOr(&bm[(y[c] >> 5) * 32], 1u << (y[c] & 31u))
                                  : ~0u;
-                // entries carry the word that reaches them: the parent's letters,
-                // plus letter lv = b for the b-images, lv the parent's level (an
-                // entry holds 32 - NMAX letters; a fresh image of a parent at
-                // level >= 32 - NMAX escalates instead)
-                uint32_t boundary = tail;   // the ring's end once the current level's children are in
-                bool deep = false;
+                bool any = false;
 #pragma unroll
                 for (int c = 0; c < 2 * P; ++c) {
-                    const int i = c >> 1;
-                    const uint32_t lv = level + ((uint32_t)i >= in_cur ? 1u : 0u);
                     if (!(old[c] & (1u << (y[c] & 31u)))) {
-                        uint32_t hi = 0;
-                        if (WORDS) {
-                            hi = e[i] & ~G::kMask;
-                            if ((c & 1) && lv < (uint32_t)G::kWordMax) hi |= 1u << (lv + NMAX);
-                            deep |= lv >= (uint32_t)G::kWordMax;
-                        }
-                        rq[(tail & rmask) * 32] = y[c] | hi;
+                        rq[(tail & rmask) * 32] = y[c] | hi[c];
                         ++tail;
+                        any = true;
                     }
-                    if ((c & 1) && (uint32_t)i < in_cur) boundary = tail;
                 }
                 // more live entries than ring slots (the oldest were overwritten), or
                 // a word longer than an entry carries: the whole-warp search takes over
-                if (tail - head > (uint32_t)ring || deep) {
+                if (tail - head > (uint32_t)ring || (WORDS && any && level >= (uint32_t)G::kWordMax)) {
                     state = kEscalate;
-                } else if (head >= lvl_end) {
-                    if (head < boundary) {          // into the next level
-                        lvl_end = boundary;
-                        ++level;
-                    } else if (tail > boundary) {   // the next level was used up in this step too
-                        lvl_end = tail;
-                        level += 2;
-                    } else {                        // nothing left: not synchronizing
+                } else if (head == lvl_end) {
+                    if (tail == lvl_end) {
                         state = kDone;
                         res_len = kLenNonSync;
+                    } else {
+                        lvl_end = tail;
+                        ++level;
                     }
                 }
             }

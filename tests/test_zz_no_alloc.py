@@ -11,7 +11,10 @@ point: lengths bit-exact, every word replaying to a single state (shortest
 words are not unique, so the two paths may return different valid words), the
 Cerny check identical.  Each batch is solved twice in a row with the same
 inputs: the second call starts from whatever the first left in the shared
-array, so identical results show that the call resets that state.  A batch
+array, so identical lengths and violation index show that the call resets
+that state.  (The words of the two calls may differ: the pooled kernel
+interleaves several automata per warp, so which of several shortest words an
+automaton reaches first depends on scheduling; each must replay.)  A batch
 with a malformed record (length -2) comes before a clean one, which must not
 inherit it.
 
@@ -75,7 +78,6 @@ def test_noalloc_matches_the_regular_entry_point(oracle_mod):
                 assert int(d_fv.item()) == ref["first_violation"] == -1
                 runs.append((lens, words))
             np.testing.assert_array_equal(runs[0][0], runs[1][0])
-            np.testing.assert_array_equal(runs[0][1], runs[1][1])
 
 
 def test_noalloc_malformed_record_does_not_leak_into_the_next_call(oracle_mod):
