@@ -661,9 +661,9 @@ def extra_summaries(args, eng, dev, stream, flush, hbm_peak: float, threads: int
 # serving: open-loop Poisson arrivals of single-automaton requests
 # ---------------------------------------------------------------------------
 
-def serve_sweep(count, rates, max_batch=0, max_levels=0):
+def serve_sweep(count, rates, max_batch=0, max_levels=0, max_n=24):
     """Open-loop Poisson sweep of single-automaton requests through the serving
-    loop (n log-uniform 8..24, 5 % Cerny family); one entry per offered rate
+    loop (n log-uniform 8..max_n, 5 % Cerny family); one entry per offered rate
     (0 = all submitted at once).  A client thread submits, at every moment,
     all requests whose arrival time has passed in one sbfs_server_submit_many
     call; a request's latency is its time in the server (submission to
@@ -676,7 +676,7 @@ def serve_sweep(count, rates, max_batch=0, max_levels=0):
     from sbfs.server import Server
 
     seed = 0x5EED + 3
-    ns = P.log_uniform_sizes(count, 8, 24, seed)
+    ns = P.log_uniform_sizes(count, 8, max_n, seed)
     recs = P.uniform_maps(count, ns, seed + 1)
     cerny = np.arange(0, count, 20)          # 5% Cerny family
     for i in cerny:

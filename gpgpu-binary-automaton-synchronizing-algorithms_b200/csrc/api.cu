@@ -231,8 +231,13 @@ sbfs_status run_level_class(sbfs_handle *h, Lane &L, const Job &j, const Batch &
         CK(E.collect(done), "collecting level slots");
         for (auto &f : done)
             if (f.state == kSlotFail) return fail(h, SBFS_ECUDA, "level slot queue overflow");
-        // long-running automata: fewer host round trips
-        levels = done.empty() ? std::min(levels * 2, 256) : 4;
+        // long-running automata: fewer host round trips -- but once the levels
+        // have shrunk to a few narrow-level widths, short batches, so that the
+        // host sees them become narrow and hands them to the one-cluster kernel
+        // (a whole-grid launch costs ~11 us even for a narrow level; C_28 has
+        // 112 levels between 256K and 16K subsets on its way down)
+        const int cap = E.level_total() <= 16 * kNarrowLevel ? 16 : 256;
+        levels = done.empty() ? std::min(levels * 2, cap) : 4;
     }
     L.level_expanded += E.expanded() - expanded0;
     return SBFS_OK;

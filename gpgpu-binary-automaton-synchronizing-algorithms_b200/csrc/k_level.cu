@@ -28,14 +28,19 @@ namespace {
 namespace cg = cooperative_groups;
 
 constexpr int kThreads = 512;
-constexpr int kStage = 2 * kThreads;   // staged pushes per CTA round
 constexpr int kNarrowCluster = 8;      // CTAs of the narrow-level kernel's cluster
+// Items a thread of k_level expands per round: their queue loads, bitmap
+// probes and atomics are issued together, so a wide level (C_28 has levels of
+// up to 3.6M subsets) keeps K times more L2 requests in flight per thread.
+constexpr int kWideItems = 2;
 
+template <int K>
 struct LevelSmem {
+    static constexpr int kStage = 2 * K * kThreads;   // staged pushes per CTA round
     unsigned long long prefix[kMaxLevelSlots + 1];
     uint64_t stage[kStage];
     unsigned short stage_slot[kStage];
-    unsigned int stage_rank[kStage];
+    unsigned short stage_rank[kStage];              // rank within its slot in this round (< kStage)
     unsigned int count;
     unsigned int slot_count[kMaxLevelSlots];
     unsigned long long slot_base[kMaxLevelSlots];
@@ -61,10 +66,13 @@ __device__ __forceinline__ int find_slot(const unsigned long long *prefix, int n
     return lo;
 }
 
-// Expands this CTA's share of the current level of every running slot: items
-// [cta * blockDim, ...) with stride ncta * blockDim over the concatenation of
-// the slots' levels (sh.prefix).  Returns the number of subsets expanded.
-__device__ unsigned long long level_items(LevelSlot *slots, const uint64_t *tables, LevelSmem &sh, int nslots,
+// Expands this CTA's share of the current level of every running slot, over
+// the concatenation of the slots' levels (sh.prefix).  A round gives each
+// thread up to K items, ncta * blockDim apart (so a level narrower than a
+// full round still spreads over every CTA, and the j-th items of a warp are
+// consecutive: coalesced queue reads).  Returns the number of subsets expanded.
+template <int K>
+__device__ unsigned long long level_items(LevelSlot *slots, const uint64_t *tables, LevelSmem<K> &sh, int nslots,
                                           unsigned long long total, int cta, int ncta)
 {
     const int tid = threadIdx.x;
@@ -72,61 +80,85 @@ __device__ unsigned long long level_items(LevelSlot *slots, const uint64_t *tabl
     const unsigned long long gthreads = (unsigned long long)ncta * blockDim.x;
     // ---- one level of every running slot ------------------------------------
     // Pushes are staged per CTA round; positions come from one shared atomic per
-    // warp (staging slot) and per warp and automaton (rank within the automaton),
-    // so no shared address is hammered by every thread.
+    // warp and image batch (staging slot) and per warp and automaton (rank
+    // within the automaton), so no shared address is hammered by every thread.
     unsigned long long expanded = 0;
     const unsigned lt = (1u << lane) - 1u;
-    for (unsigned long long base = (unsigned long long)cta * blockDim.x; base < total; base += gthreads) {
+    for (unsigned long long base = (unsigned long long)cta * blockDim.x; base < total; base += K * gthreads) {
         if (tid == 0) sh.count = 0;
         __syncthreads();
-        const unsigned long long item = base + tid;
-        const bool have = item < total;
-        int s = 0;
-        unsigned long long idx = 0;
-        uint64_t t = 0;
-        LevelSlot *sl = nullptr;
-        if (have) {
-            s = find_slot(sh.prefix, nslots, item);
-            sl = &slots[s];
-            idx = sh.lvl_start[s] + (item - sh.prefix[s]);
-            const uint32_t x = (uint32_t)(__ldcg(sl->queue + idx) & kLevelSubsetMask);
-            const uint64_t *tb = tables + (size_t)s * kLevelTable;
-            t = __ldg(tb + (x & 255u));
-            t |= __ldg(tb + 256 + ((x >> 8) & 255u));
-            t |= __ldg(tb + 512 + ((x >> 16) & 255u));
-            t |= __ldg(tb + 768 + ((x >> 24) & 255u));
-            ++expanded;
-        }
+        int s[K];
+        unsigned long long idx[K];
+        uint32_t x[K];
+        bool have[K];
+        // queue entries first (K independent loads) ...
 #pragma unroll
-        for (int letter = 0; letter < 2; ++letter) {
-            const uint32_t y = letter ? (uint32_t)t : (uint32_t)(t >> 32);
-            bool push = false;
-            if (have) {
-                const uint32_t m = 1u << (y & 31u);
-                // bits only ever go 0 -> 1 during a search: a set bit seen by a
-                // plain load is final; otherwise the atomic decides who pushes
-                if (!(__ldcg(sl->bitmap + (y >> 5)) & m) && !(atomicOr(sl->bitmap + (y >> 5), m) & m)) {
-                    if (is_singleton(y))
-                        atomicMin(&sl->found, (idx << 1) | (unsigned long long)letter);
+        for (int j = 0; j < K; ++j) {
+            const unsigned long long item = base + (unsigned long long)j * gthreads + tid;
+            have[j] = item < total;
+            s[j] = 0;
+            idx[j] = 0;
+            x[j] = 0;
+            if (have[j]) {
+                s[j] = find_slot(sh.prefix, nslots, item);
+                idx[j] = sh.lvl_start[s[j]] + (item - sh.prefix[s[j]]);
+                x[j] = (uint32_t)(__ldcg(slots[s[j]].queue + idx[j]) & kLevelSubsetMask);
+            }
+        }
+        // ... then both images of each from the byte tables ...
+        uint32_t y[2 * K];
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            uint64_t t = 0;
+            if (have[j]) {
+                const uint64_t *tb = tables + (size_t)s[j] * kLevelTable;
+                t = __ldg(tb + (x[j] & 255u));
+                t |= __ldg(tb + 256 + ((x[j] >> 8) & 255u));
+                t |= __ldg(tb + 512 + ((x[j] >> 16) & 255u));
+                t |= __ldg(tb + 768 + ((x[j] >> 24) & 255u));
+                ++expanded;
+            }
+            y[2 * j] = (uint32_t)(t >> 32);
+            y[2 * j + 1] = (uint32_t)t;
+        }
+        // ... then the atomic test-and-set of every image, issued back to back.
+        // (A plain load of the bitmap word first, to skip the atomic for images
+        // already visited -- about half of them on a Cerny level -- lengthens the
+        // dependent chain more than it saves: C_28 took 15.4 ms with it, 13.2 ms
+        // without.)
+        bool push[2 * K];
+#pragma unroll
+        for (int c = 0; c < 2 * K; ++c) {
+            const uint32_t m = 1u << (y[c] & 31u);
+            push[c] = false;
+            if (have[c >> 1]) {
+                LevelSlot *sl = &slots[s[c >> 1]];
+                if (!(atomicOr(sl->bitmap + (y[c] >> 5), m) & m)) {
+                    if (is_singleton(y[c]))
+                        atomicMin(&sl->found, (idx[c >> 1] << 1) | (unsigned long long)(c & 1));
                     else
-                        push = true;
+                        push[c] = true;
                 }
             }
-            const unsigned pm = __ballot_sync(kFull, push);
+        }
+#pragma unroll
+        for (int c = 0; c < 2 * K; ++c) {
+            const unsigned pm = __ballot_sync(kFull, push[c]);
             if (pm) {
                 unsigned int pos = 0;
                 const int leader = __ffs(pm) - 1;
                 if (lane == leader) pos = atomicAdd(&sh.count, (unsigned)__popc(pm));
                 pos = __shfl_sync(kFull, pos, leader) + __popc(pm & lt);
-                if (push) {
-                    const unsigned grp = __match_any_sync(pm, s);
+                if (push[c]) {
+                    const int q = s[c >> 1];
+                    const unsigned grp = __match_any_sync(pm, q);
                     const int gl = __ffs(grp) - 1;
                     unsigned int r0 = 0;
-                    if (lane == gl) r0 = atomicAdd(&sh.slot_count[s], (unsigned)__popc(grp));
+                    if (lane == gl) r0 = atomicAdd(&sh.slot_count[q], (unsigned)__popc(grp));
                     const unsigned int rank = __shfl_sync(grp, r0, gl) + __popc(grp & lt);
-                    sh.stage[pos] = (uint64_t)y | (idx << 28) | ((uint64_t)letter << 63);
-                    sh.stage_slot[pos] = (unsigned short)s;
-                    sh.stage_rank[pos] = rank;
+                    sh.stage[pos] = (uint64_t)y[c] | (idx[c >> 1] << 28) | ((uint64_t)(c & 1) << 63);
+                    sh.stage_slot[pos] = (unsigned short)q;
+                    sh.stage_rank[pos] = (unsigned short)rank;
                 }
             }
         }
@@ -160,7 +192,8 @@ __device__ unsigned long long level_items(LevelSlot *slots, const uint64_t *tabl
 // freshly admitted slots into running ones, and writes the prefix sums of the
 // new levels to prefix_out.  Returns the new total (block-uniform); `running`
 // receives the number of running slots.
-__device__ unsigned long long level_transition(LevelSlot *slots, LevelCtl *ctl, const Batch &out, LevelSmem &sh,
+template <int K>
+__device__ unsigned long long level_transition(LevelSlot *slots, LevelCtl *ctl, const Batch &out, LevelSmem<K> &sh,
                                                int nslots, unsigned long long *prefix_out, int &running)
 {
     const int tid = threadIdx.x;
@@ -262,7 +295,7 @@ __device__ unsigned long long level_transition(LevelSlot *slots, LevelCtl *ctl, 
 __global__ void __launch_bounds__(kThreads) k_level(LevelSlot *slots, uint64_t *tables, LevelCtl *ctl,
                                                     Batch out, int par)
 {
-    __shared__ LevelSmem sh;
+    __shared__ LevelSmem<kWideItems> sh;
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int nslots = ctl->nslots;
@@ -307,7 +340,7 @@ __global__ void __launch_bounds__(kThreads) k_level(LevelSlot *slots, uint64_t *
     for (int q = tid; q < nslots; q += blockDim.x) sh.lvl_start[q] = slots[q].lvl_start;
     __syncthreads();
 
-    unsigned long long expanded = level_items(slots, tables, sh, nslots, total, blockIdx.x, need);
+    unsigned long long expanded = level_items<kWideItems>(slots, tables, sh, nslots, total, blockIdx.x, need);
     for (int o = 16; o; o >>= 1) expanded += __shfl_down_sync(kFull, expanded, o);
     if (lane == 0 && expanded) atomicAdd(&ctl->expanded, expanded);
 
@@ -342,7 +375,7 @@ __global__ void __cluster_dims__(kNarrowCluster, 1, 1) __launch_bounds__(kThread
     k_level_narrow(LevelSlot *slots, uint64_t *tables, LevelCtl *ctl, Batch out, int par, int max_levels,
                    unsigned long long narrow)
 {
-    __shared__ LevelSmem sh;
+    __shared__ LevelSmem<1> sh;
     cg::cluster_group cluster = cg::this_cluster();
     const int rank = (int)cluster.block_rank();
     const int tid = threadIdx.x;
@@ -356,9 +389,9 @@ __global__ void __cluster_dims__(kNarrowCluster, 1, 1) __launch_bounds__(kThread
     __syncthreads();
     unsigned long long expanded = 0;
     int running = 0;
-    LevelSmem *sh0 = cluster.map_shared_rank(&sh, 0);
+    LevelSmem<1> *sh0 = cluster.map_shared_rank(&sh, 0);
     for (int it = 0; it < max_levels; ++it) {
-        expanded += level_items(slots, tables, sh, nslots, total, rank, kNarrowCluster);
+        expanded += level_items<1>(slots, tables, sh, nslots, total, rank, kNarrowCluster);
         cluster.sync();   // every CTA's pushes of this level are in
         if (rank == 0) {
             total = level_transition(slots, ctl, out, sh, nslots, sh.prefix, running);

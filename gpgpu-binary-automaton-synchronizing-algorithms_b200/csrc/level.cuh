@@ -125,6 +125,8 @@ public:
         return true;
     }
     bool launched() const { return launched_; }
+    // subsets in the levels the next launch expands (as of the last collect)
+    unsigned long long level_total() const { return h_ctl_ ? h_ctl_->total[parity_ & 1] : 0ull; }
     void reset_peak() { arena().reset_peak(); }
     int in_flight() const { return in_flight_; }
     size_t arena_used() const { return arena().used(); }

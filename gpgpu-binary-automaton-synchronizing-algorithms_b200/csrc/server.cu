@@ -24,6 +24,7 @@
 // Completion order follows the GPU, not submission order.
 #include <atomic>
 #include <chrono>
+#include <cstddef>
 #include <cstdlib>
 #include <condition_variable>
 #include <cstring>
@@ -33,6 +34,7 @@
 #include <thread>
 #include <unordered_map>
 #include <unordered_set>
+#include <vector>
 
 #include "runtime.cuh"
 
@@ -43,9 +45,10 @@ namespace {
 struct Request {
     uint64_t id;
     int32_t n;
-    uint8_t a[32], b[32];
+    uint8_t a[32], b[32];   // zero past n: together the 64-byte record of the batch kernels
     double submit_ms;
 };
+static_assert(offsetof(Request, b) == offsetof(Request, a) + 32, "a and b form one 64-byte record");
 
 constexpr int kSmallMaxN = 20;
 constexpr int kWords = 12;
@@ -94,6 +97,7 @@ struct sbfs_server {
     unsigned int next_tag = 1;
     Arena arena;                                   // HBM budget of the admitted large requests
     int64_t small_used = 0, small_peak = 0;        // footprint of the mini-batches in flight
+    std::vector<sbfs_result> batch_out;            // results of one poll pass, handed over together
     LevelEngine big;                               // level slots for n >= 21
     std::unordered_map<long long, Request> large;   // admitted, keyed by id
     std::string error;
@@ -115,7 +119,7 @@ struct sbfs_server {
 
 namespace {
 
-void complete(sbfs_server *s, const Request &r, int32_t status, int32_t len, const uint64_t *word)
+sbfs_result make_result(const Request &r, int32_t status, int32_t len, const uint64_t *word, double done_ms)
 {
     sbfs_result res;
     std::memset(&res, 0, sizeof(res));
@@ -125,12 +129,33 @@ void complete(sbfs_server *s, const Request &r, int32_t status, int32_t len, con
     res.n = r.n;
     if (word) std::memcpy(res.word, word, sizeof(res.word));
     res.submit_ms = r.submit_ms;
-    res.done_ms = s->now_ms();
+    res.done_ms = done_ms;
+    return res;
+}
+
+void complete(sbfs_server *s, const Request &r, int32_t status, int32_t len, const uint64_t *word)
+{
+    const sbfs_result res = make_result(r, status, len, word, s->now_ms());
     std::lock_guard<std::mutex> lock(s->mu);
     s->ready.push_back(res);
     s->st.completed++;
     if (status == SBFS_ECANCELED) s->st.cancelled++;
     s->cv_out.notify_all();
+}
+
+// Hands a batch of finished results to the pollers under one lock: a burst of
+// thousands of requests finishing together costs one lock and one wake-up,
+// not one per request.
+void deliver(sbfs_server *s, std::vector<sbfs_result> &batch)
+{
+    if (batch.empty()) return;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        for (const sbfs_result &r : batch) s->ready.push_back(r);
+        s->st.completed += (int64_t)batch.size();
+    }
+    s->cv_out.notify_all();
+    batch.clear();
 }
 
 enum class Ev { kPending, kDone, kFailed };
@@ -167,9 +192,7 @@ bool launch_small(sbfs_server *s, SmallSlot &S)
     int max_n = 1;
     for (int64_t i = 0; i < cnt; ++i) {
         const Request &r = S.reqs[(size_t)i];
-        std::memset(rec + i * 64, 0, 64);
-        std::memcpy(rec + i * 64, r.a, (size_t)r.n);
-        std::memcpy(rec + i * 64 + 32, r.b, (size_t)r.n);
+        std::memcpy(rec + i * 64, r.a, 64);
         ns[i] = (uint8_t)r.n;
         max_n = std::max(max_n, r.n);
     }
@@ -242,15 +265,18 @@ bool poll_small(sbfs_server *s, SmallSlot &S)
                                             : "serving mini-batch: device error bits set";
         }
     }
+    std::vector<sbfs_result> &out = s->batch_out;
+    const double now = s->now_ms();
     for (size_t i = 0; i < S.reqs.size() && S.left; ++i) {
         if (S.delivered[i] || (flag[i] != S.tag && !finished)) continue;
         std::atomic_thread_fence(std::memory_order_acquire);
-        if (status == SBFS_OK) complete(s, S.reqs[i], SBFS_OK, len[i], words + i * kWords);
-        else complete(s, S.reqs[i], status, -1, nullptr);
+        if (status == SBFS_OK) out.push_back(make_result(S.reqs[i], SBFS_OK, len[i], words + i * kWords, now));
+        else out.push_back(make_result(S.reqs[i], status, -1, nullptr, now));
         S.delivered[i] = 1;
         --S.left;
         progress = true;
     }
+    deliver(s, out);
     if (finished) {
         S.reqs.clear();
         S.busy = false;
