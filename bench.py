@@ -571,9 +571,11 @@ def run_sbfs(args):
                             "p99_ms_all": e["latency_ms"]["p99"], "client_lag_ms_p99": e["client_lag_ms_p99"],
                             "peak_hbm_admitted_bytes": e["peak_arena_bytes"] + e["peak_small_footprint_bytes"],
                             "statuses_ok": e["statuses_ok"]}
+                # 100K requests at two Poisson rates and as one burst, then a 10K burst
+                sweep = serve_sweep(args.serving_requests, [32000.0, 256000.0, 0.0])
+                sweep += serve_sweep(10_000, [0.0])
                 line["serving"] = {"requests": args.serving_requests,
-                                   "sweep": [brief(e) for e in serve_sweep(args.serving_requests,
-                                                                           [32000.0, 256000.0, 0.0])],
+                                   "sweep": [dict(brief(e), requests=e["requests"]) for e in sweep],
                                    "full_sweep": "bench.py --workload serving"}
             if not args.no_extra:
                 line.update(extra_summaries(args, eng, dev, stream, flush, hbm_peak, threads))

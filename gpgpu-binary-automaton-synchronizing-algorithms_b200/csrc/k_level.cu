@@ -48,6 +48,7 @@ struct LevelSmem {
     unsigned long long lvl_start[kMaxLevelSlots];   // current level's first queue index per slot
     unsigned long long b_total;                     // narrow kernel: rank 0's transition results
     int b_running;
+    int b_it;                                       // narrow kernel: levels run so far
     bool last;
 };
 
@@ -370,7 +371,10 @@ __global__ void __launch_bounds__(kThreads) k_level(LevelSlot *slots, uint64_t *
 // to its next level, the others take the new prefix sums from rank 0's shared
 // memory -- with hardware cluster barriers instead of launches between levels,
 // while the levels stay at most `narrow` subsets wide, up to `max_levels`
-// levels.  Launched as one cluster, and only when no slot awaits set-up.
+// levels.  Levels of at most one CTA round (the Cerny automata's long tails:
+// 289 of C_28's levels have at most 512 subsets) are run by rank 0 alone with
+// CTA barriers, the other CTAs waiting at one cluster barrier (C_28 12.8 ->
+// 12.5 ms).  Launched as one cluster, and only when no slot awaits set-up.
 __global__ void __cluster_dims__(kNarrowCluster, 1, 1) __launch_bounds__(kThreads)
     k_level_narrow(LevelSlot *slots, uint64_t *tables, LevelCtl *ctl, Batch out, int par, int max_levels,
                    unsigned long long narrow)
@@ -390,7 +394,40 @@ __global__ void __cluster_dims__(kNarrowCluster, 1, 1) __launch_bounds__(kThread
     unsigned long long expanded = 0;
     int running = 0;
     LevelSmem<1> *sh0 = cluster.map_shared_rank(&sh, 0);
-    for (int it = 0; it < max_levels; ++it) {
+    int it = 0;
+    while (it < max_levels) {
+        if (total <= (unsigned long long)kThreads) {
+            // levels of at most one round: rank 0 runs them by itself with CTA
+            // barriers only, while the other CTAs wait at one cluster barrier
+            if (rank == 0) {
+                while (it < max_levels) {
+                    expanded += level_items<1>(slots, tables, sh, nslots, total, 0, 1);
+                    __syncthreads();
+                    total = level_transition(slots, ctl, out, sh, nslots, sh.prefix, running);
+                    for (int q = tid; q < nslots; q += blockDim.x) sh.lvl_start[q] = slots[q].lvl_start;
+                    __syncthreads();
+                    ++it;
+                    if (running == 0 || total > (unsigned long long)kThreads) break;
+                }
+                if (tid == 0) {
+                    sh.b_total = total;
+                    sh.b_running = running;
+                    sh.b_it = it;
+                }
+            }
+            cluster.sync();   // rank 0's levels are done and its results visible
+            if (rank != 0) {
+                for (int i = tid; i <= nslots; i += blockDim.x) sh.prefix[i] = sh0->prefix[i];
+                for (int q = tid; q < nslots; q += blockDim.x) sh.lvl_start[q] = sh0->lvl_start[q];
+            }
+            total = sh0->b_total;
+            running = sh0->b_running;
+            it = sh0->b_it;
+            __syncthreads();
+            cluster.sync();   // every CTA has read rank 0's results before rank 0 writes again
+            if (running == 0 || total > narrow) break;
+            continue;
+        }
         expanded += level_items<1>(slots, tables, sh, nslots, total, rank, kNarrowCluster);
         cluster.sync();   // every CTA's pushes of this level are in
         if (rank == 0) {
@@ -413,6 +450,7 @@ __global__ void __cluster_dims__(kNarrowCluster, 1, 1) __launch_bounds__(kThread
             total = sh.b_total;
             running = sh.b_running;
         }
+        ++it;
         if (running == 0 || total > narrow) break;
     }
     for (int o = 16; o; o >>= 1) expanded += __shfl_down_sync(kFull, expanded, o);
