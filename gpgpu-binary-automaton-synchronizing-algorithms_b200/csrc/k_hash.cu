@@ -235,224 +235,6 @@ __global__ void __launch_bounds__(HashGeom<CAP_BITS>::kWarps * 32)
     if (lane == 0 && b.expanded && expanded) atomicAdd(b.expanded, expanded);
 }
 
-// Two automata per warp: each 16-lane half of the warp searches its own
-// automaton with its own tables, hash set and queue, exactly as k_hash does
-// with a whole warp.  An automaton's first levels are narrower than 32 subsets
-// (a random one with 13..20 states has about 11 levels of a few to a few
-// hundred subsets), so a whole warp per automaton leaves about half of its
-// lanes idle; two halves fill them.  The halves step together (one warp
-// instruction stream, with per-half predicates), so every ballot and shuffle
-// below involves the whole warp and no half ever waits for the other inside
-// a search.
-template <int CAP_BITS>
-struct __align__(16) HashHalf {
-    uint64_t table[5 * 16];
-    uint32_t set[1 << CAP_BITS];
-    uint16_t queue[(3u << CAP_BITS) / 4u];   // set slot | letter-is-b << 15
-    uint16_t parent[(3u << CAP_BITS) / 4u];
-};
-
-template <int CAP_BITS>
-struct Hash2Geom {
-    static constexpr int kCap = 1 << CAP_BITS;
-    static constexpr uint32_t kLimit = 3u * (1u << CAP_BITS) / 4u;
-    static constexpr int kWarps = 7;   // 7 warps x 2 halves per CTA
-};
-
-template <int CAP_BITS>
-__global__ void __launch_bounds__(Hash2Geom<CAP_BITS>::kWarps * 32)
-    k_hash2(Batch b, int32_t *heavy_list, unsigned long long *heavy_count, unsigned long long *ticket)
-{
-    using G = Hash2Geom<CAP_BITS>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    const int half = lane >> 4, hl = lane & 15;
-    const int hbase = lane & 16;                    // first lane of this half
-    HashHalf<CAP_BITS> &W = reinterpret_cast<HashHalf<CAP_BITS> *>(smem_raw)[2 * warp + half];
-    int64_t count;
-    const int32_t *order;
-    resolve_work(b, count, order);
-    for (int i = hl; i < G::kCap; i += 16) W.set[i] = 0u;
-    __syncwarp();
-    uint32_t gen = 0;                               // per half: this automaton's set generation
-    unsigned long long expanded = 0;
-    bool more = true;                               // the batch may hold more automata (warp-uniform)
-    bool run = false;                               // this half searches an automaton (half-uniform)
-    int64_t k = -1;
-    int n = 0;
-    uint32_t head = 0, lvl_end = 0, tail = 0, level = 0;
-    const unsigned lt = (1u << hl) - 1u;            // lanes below this one in its half
-
-    while (true) {
-        // ---- halves without an automaton take the next ones (one ticket atomic)
-        const unsigned wm = __ballot_sync(kFull, !run && hl == 0);   // lane 0 / 16 of each idle half
-        if (more && wm) {
-            unsigned long long got = 0;
-            const int leader = __ffs(wm) - 1;
-            if (lane == leader) got = atomicAdd(ticket, (unsigned long long)__popc(wm));
-            got = __shfl_sync(kFull, got, leader);
-            if (got + __popc(wm) >= (unsigned long long)count) more = false;
-            const bool want = (wm >> hbase) & 1u;
-            const unsigned long long pos = got + ((half == 1 && (wm & 1u)) ? 1u : 0u);
-            bool start = want && pos < (unsigned long long)count;
-            bool bad = false;
-            uint64_t s0 = 0, s1 = 0;                // states hl and hl + 16 of this half's automaton
-            if (start) {
-                k = automaton_at(order, (int64_t)pos);
-                n = automaton_n(b, k);
-                bad = n < 1 || n > 20 || n > b.lstride;
-                if (!bad) {
-                    const uint8_t *rec = b.maps + (size_t)k * 2u * (size_t)b.lstride;
-                    if (hl < n) {
-                        const uint32_t av = rec[hl], bv = rec[b.lstride + hl];
-                        if (av >= (uint32_t)n || bv >= (uint32_t)n) bad = true;
-                        else s0 = ((uint64_t)(1u << av) << 32) | (1u << bv);
-                    }
-                    if (hl + 16 < n) {
-                        const uint32_t av = rec[hl + 16], bv = rec[b.lstride + hl + 16];
-                        if (av >= (uint32_t)n || bv >= (uint32_t)n) bad = true;
-                        else s1 = ((uint64_t)(1u << av) << 32) | (1u << bv);
-                    }
-                }
-            }
-            const unsigned badm = __ballot_sync(kFull, bad);
-            if (start && ((badm >> hbase) & 0xFFFFu)) {
-                if (hl == 0) {
-                    record_result(b, k, n, kLenInvalid);
-                    if (b.out_words)
-                        for (int c = 0; c < b.word_stride; ++c) b.out_words[(size_t)k * b.word_stride + c] = 0ull;
-                    atomicOr(b.error, kErrInvalid);
-                    publish_result(b, k);
-                }
-                start = false;
-            }
-            // nibble tables: 80 entries per half, 5 passes of 16 lanes; every lane
-            // takes every pass (the shuffles read the whole warp)
-#pragma unroll
-            for (int pass = 0; pass < 5; ++pass) {
-                uint64_t acc = 0;
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const int st = 4 * pass + j;
-                    const uint64_t v0 = __shfl_sync(kFull, s0, hbase | (st & 15));
-                    const uint64_t v1 = __shfl_sync(kFull, s1, hbase | (st & 15));
-                    if (((hl >> j) & 1) && st < n) acc |= st < 16 ? v0 : v1;
-                }
-                if (start) W.table[pass * 16 + hl] = acc;
-            }
-            if (start && ++gen == (1u << 12)) {   // generations wrapped: clear once, start again at 1
-                for (int i = hl; i < G::kCap; i += 16) W.set[i] = 0u;
-                gen = 1;
-            }
-            __syncwarp();
-            if (start) {
-                const uint32_t full = (1u << n) - 1u;
-                if (hl == 0) W.queue[0] = (uint16_t)set_insert<CAP_BITS>(W.set, full, gen);
-                // n = 1: the visited root is the only singleton, the search generates nothing new
-                head = 0;
-                lvl_end = n > 1 ? 1u : 0u;
-                tail = lvl_end;
-                level = 0;
-                run = true;
-            }
-            __syncwarp();
-        }
-        if (!__any_sync(kFull, run)) {
-            if (!more) break;
-            continue;
-        }
-        // ---- one step of every searching half: 16 subsets of its current level
-        const uint32_t idx = head + (uint32_t)hl;
-        const bool has = run && idx < lvl_end;
-        uint32_t ya = 0, yb = 0;
-        if (has) {
-            const uint32_t x = W.set[W.queue[idx] & 0x7FFFu] & kSubsetMask;
-            const uint64_t t = W.table[x & 15u] | W.table[16 + ((x >> 4) & 15u)] | W.table[32 + ((x >> 8) & 15u)] |
-                               W.table[48 + ((x >> 12) & 15u)] | W.table[64 + ((x >> 16) & 15u)];
-            ya = (uint32_t)(t >> 32);
-            yb = (uint32_t)t;
-        }
-        expanded += has ? 1u : 0u;
-        const bool sa = has && is_singleton(ya), sb = has && is_singleton(yb);
-        const unsigned hs = (__ballot_sync(kFull, sa || sb) >> hbase) & 0xFFFFu;
-        // the first singleton in queue order (lowest lane of the half, a before b)
-        const uint32_t fletter = (uint32_t)__shfl_sync(kFull, sa ? 0 : 1, hs ? hbase + __ffs(hs) - 1 : lane);
-        bool finished = false, heavy = false;
-        int32_t len = kLenNonSync;
-        uint32_t found = 0, found_letter = 0;
-        if (run && hs) {
-            found = head + (uint32_t)(__ffs(hs) - 1);
-            found_letter = fletter;
-            len = (int32_t)level + 1;
-            finished = true;
-        }
-        const bool go = has && !hs;
-        const int sa_slot = go ? set_insert<CAP_BITS>(W.set, ya, gen) : -1;
-        const int sb_slot = go ? set_insert<CAP_BITS>(W.set, yb, gen) : -1;
-        bool fa = sa_slot >= 0, fb = sb_slot >= 0;
-        const unsigned ma = (__ballot_sync(kFull, fa) >> hbase) & 0xFFFFu;
-        const unsigned mb = (__ballot_sync(kFull, fb) >> hbase) & 0xFFFFu;
-        const uint32_t added = (uint32_t)(__popc(ma) + __popc(mb));
-        const bool stepping = run && !hs;
-        if (stepping && tail + added > G::kLimit) heavy = true;
-        if (go && !heavy) {
-            uint32_t p = tail + (uint32_t)(__popc(ma & lt) + __popc(mb & lt));
-            if (!SBFS_CHECK(p + (fa ? 1u : 0u) + (fb ? 1u : 0u) <= G::kLimit, b.error)) fa = fb = false;
-            if (fa) {
-                W.queue[p] = (uint16_t)sa_slot;
-                W.parent[p++] = (uint16_t)idx;
-            }
-            if (fb) {
-                W.queue[p] = (uint16_t)(sb_slot | 0x8000);
-                W.parent[p] = (uint16_t)idx;
-            }
-        }
-        if (stepping && !heavy) {
-            tail += added;
-            head = min(head + 16u, lvl_end);
-        }
-        __syncwarp();
-        if (stepping && !heavy && head == lvl_end) {
-            if (tail == lvl_end) {
-                finished = true;             // no new subset: not synchronizing
-            } else {
-                lvl_end = tail;
-                if (++level >= kHashLevelCap) heavy = true;
-            }
-        }
-        if (heavy) {
-            // a long or wide search: the CTA-wide kernel takes it from the start
-            if (hl == 0) heavy_list[atomicAdd(heavy_count, 1ull)] = (int32_t)k;
-            run = false;
-        } else if (finished) {
-            if (hl == 0) {
-                record_result(b, k, n, len);
-                if (b.out_words) {
-                    // letters from the root: the entry at depth d + 1 holds letter d
-                    uint64_t w0 = 0;
-                    if (len > 0) {
-                        if (found_letter) w0 |= 1ull << level;
-                        uint32_t i = found;
-                        for (int d = (int)level - 1; d >= 0; --d) {
-                            if (W.queue[i] >> 15) w0 |= 1ull << d;
-                            i = W.parent[i];
-                        }
-                    }
-                    uint64_t *w = b.out_words + (size_t)k * (size_t)b.word_stride;
-                    w[0] = w0;
-                    for (int c = 1; c < b.word_stride; ++c) w[c] = 0ull;
-                }
-                publish_result(b, k);
-            }
-            run = false;
-        }
-        __syncwarp();
-    }
-    for (int o = 16; o; o >>= 1) expanded += __shfl_down_sync(kFull, expanded, o);
-    if (lane == 0 && b.expanded && expanded) atomicAdd(b.expanded, expanded);
-}
-
 // Counting sort of a hand-off list by n, largest first (one CTA): the
 // persistent CTA-wide kernel then takes the longest searches first, and the
 // short ones fill the SMs that free up (longest-processing-time order).
@@ -556,67 +338,12 @@ struct HashLaunch {
     }
 };
 
-// the same set-up and occupancy bookkeeping for the two-automata-per-warp kernel
-template <int CAP_BITS>
-struct Hash2Launch {
-    static size_t smem() { return (size_t)Hash2Geom<CAP_BITS>::kWarps * 2 * sizeof(HashHalf<CAP_BITS>); }
-    static cudaError_t prepare()
-    {
-        static std::atomic<int> done[kMaxDevices];
-        const int dev = current_device();
-        const bool cached = dev >= 0 && dev < kMaxDevices;
-        if (cached && done[dev].load(std::memory_order_acquire)) return cudaSuccess;
-        const cudaError_t e =
-            cudaFuncSetAttribute(k_hash2<CAP_BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem());
-        if (e == cudaSuccess && cached) done[dev].store(1, std::memory_order_release);
-        return e;
-    }
-    static int per_sm()
-    {
-        static std::atomic<int> known[kMaxDevices];
-        const int dev = current_device();
-        const bool cached = dev >= 0 && dev < kMaxDevices;
-        if (cached) {
-            const int v = known[dev].load(std::memory_order_relaxed);
-            if (v > 0) return v;
-        }
-        if (prepare() != cudaSuccess) {
-            cudaGetLastError();
-            return 0;
-        }
-        int blocks = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_hash2<CAP_BITS>,
-                                                          Hash2Geom<CAP_BITS>::kWarps * 32, smem()) != cudaSuccess) {
-            cudaGetLastError();
-            return 0;
-        }
-        if (cached && blocks > 0) known[dev].store(blocks, std::memory_order_relaxed);
-        return blocks;
-    }
-    static cudaError_t launch(int ctas, const Batch &b, int32_t *list, unsigned long long *count,
-                              unsigned long long *ticket, cudaStream_t st)
-    {
-        cudaError_t e = prepare();
-        if (e != cudaSuccess) return e;
-        k_hash2<CAP_BITS><<<ctas, Hash2Geom<CAP_BITS>::kWarps * 32, smem(), st>>>(b, list, count, ticket);
-        return cudaGetLastError();
-    }
-};
-
 }  // namespace
 
-// size 1: one automaton per warp, 2048 hash slots (1536 subsets); size 2: 4096
-// slots (3072 subsets); size 3: two automata per warp, 2048 slots each; size 4:
-// two per warp, 1024 slots each (768 subsets)
+// size 1: 2048 hash slots per warp (1536 subsets), size 2: 4096 (3072 subsets)
 int hash_max_ctas_per_sm(int size)
 {
-    switch (size) {
-    case 1: return HashLaunch<11>::per_sm();
-    case 2: return HashLaunch<12>::per_sm();
-    case 3: return Hash2Launch<11>::per_sm();
-    case 4: return Hash2Launch<10>::per_sm();
-    }
-    return 0;
+    return size == 2 ? HashLaunch<12>::per_sm() : size == 1 ? HashLaunch<11>::per_sm() : 0;
 }
 
 cudaError_t launch_sort_handoff(const Batch &b, const int32_t *list, const unsigned long long *count, int32_t *out,
@@ -632,8 +359,6 @@ cudaError_t launch_hash(int size, int ctas, const Batch &b, int32_t *heavy_list,
     if (ctas < 1 || !heavy_list || !heavy_count) return cudaErrorInvalidValue;
     if (size == 1) return HashLaunch<11>::launch(ctas, b, heavy_list, heavy_count, ticket, st);
     if (size == 2) return HashLaunch<12>::launch(ctas, b, heavy_list, heavy_count, ticket, st);
-    if (size == 3) return Hash2Launch<11>::launch(ctas, b, heavy_list, heavy_count, ticket, st);
-    if (size == 4) return Hash2Launch<10>::launch(ctas, b, heavy_list, heavy_count, ticket, st);
     return cudaErrorInvalidValue;
 }
 
