@@ -531,6 +531,12 @@ def run_sbfs(args):
                         "algorithmic_bytes": f"records + results + {LEVEL_BYTES_PER_EXPANSION} B per expansion "
                                              "(HBM bitmaps and queues)",
                         "expansions_per_launch": expanded_per_step}
+            l2_peak = onchip_cal.get("l2_random_atomic_gops")
+            atom = 2 * expanded_per_step / (ms / 1e3) / 1e9
+            roofline["l2_atomics"] = {"achieved": atom, "peak": l2_peak, "unit": "G atomicOr/s",
+                                      "frac": atom / l2_peak if l2_peak else None, "per_expansion": 2,
+                                      "peak_source": "measured random atomicOr on an L2-resident 32 MiB bitmap "
+                                                     "(profiles/onchip.json)"}
         else:
             achieved = expanded_per_step * SMEM_BYTES_PER_EXPANSION / (ms / 1e3) / 1e9
             roofline = {"bound": "smem", "achieved": achieved, "peak": smem_peak, "unit": "GB/s",
@@ -622,11 +628,18 @@ def extra_summaries(args, eng, dev, stream, flush, hbm_peak: float, threads: int
     ms = statistics.mean(ms_l)
     search = int(st["expanded"]) * LEVEL_BYTES_PER_EXPANSION
     gbs = search / (ms / 1e3) / 1e9
+    # the bitmaps stay in L2: every image is one random atomicOr there, against the
+    # measured random-atomic throughput of an L2-resident 32 MiB bitmap
+    l2_peak = load_profile_json("onchip.json").get("l2_random_atomic_gops")
+    atom = 2 * int(st["expanded"]) / (ms / 1e3) / 1e9
     ref, cpu = cpu_leg(wl)
     out["large"] = {"workload": wl["desc"], "ms_per_step": ms, "automata_per_s": wl["count"] / (ms / 1e3),
                     "expansions_per_step": int(st["expanded"]),
                     "hbm_search": {"achieved": gbs, "peak": hbm_peak, "unit": "GB/s", "frac": gbs / hbm_peak,
                                    "algorithmic_bytes": f"{LEVEL_BYTES_PER_EXPANSION} B per expansion"},
+                    "l2_atomics": {"achieved": atom, "peak": l2_peak, "unit": "G atomicOr/s",
+                                   "frac": atom / l2_peak if l2_peak else None,
+                                   "per_expansion": 2, "peak_source": "measured (profiles/onchip.json)"},
                     "lengths_match_cpu": bool(np.array_equal(leg.d_len.cpu().numpy(), ref)),
                     "cpu_baseline": cpu, "steps": max(2, steps // 2)}
     del leg
