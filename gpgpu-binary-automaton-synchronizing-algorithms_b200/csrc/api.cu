@@ -736,6 +736,13 @@ sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstr
        "launching per-lane kernel");
     CK(cudaEventRecord(L.ev_k1, L.stream), "recording event");
     o.launches += 1;
+    // Every chunk copy is enqueued before anything else is launched behind the
+    // kernel: the kernel waits for those chunks, and the first launch of a
+    // kernel whose module is not loaded yet (CUDA loads modules lazily) can
+    // block this thread until the device is idle -- which the running kernel
+    // would then wait out to its bounded limit.
+    for (int64_t ci = 1; ci < nch; ++ci)
+        if ((st = copy_chunk_in(ci))) return st;
     if (out_len) {
         CK(launch_count_sync(b.out_len, cnt, &ctr->synchronizing, h->sm_count, L.stream), "launching result count");
         o.launches += 1;
@@ -743,8 +750,6 @@ sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstr
     CK(cudaMemcpyAsync(L.h_counters.ptr, L.counters.ptr, sizeof(DevCounters), cudaMemcpyDeviceToHost, L.stream),
        "copying counters");
     CK(cudaEventRecord(S.ev_kdone, L.stream), "recording event");
-    for (int64_t ci = 1; ci < nch; ++ci)
-        if ((st = copy_chunk_in(ci))) return st;
     // results out, chunk by chunk, as the kernel finishes them
     auto copy_chunk_out = [&](int64_t ci) -> sbfs_status {
         const int64_t a = ci * kStreamChunk, m = std::min(kStreamChunk, cnt - a);

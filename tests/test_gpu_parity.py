@@ -495,3 +495,32 @@ def test_config5_large_instances_as_named(engine, oracle_mod):
         idx = np.nonzero(wl["ns"] == n)[0]
         assert r["len"][idx[64]] == (n - 1) ** 2              # C_n
     assert (ref["len"] >= 0).sum() > 100
+
+
+def test_streamed_batch_as_a_fresh_process_first_call(oracle_mod, tmp_path):
+    """A process whose very first call is a streamed batch (uniform n <= 12, at
+    least 2^18 automata, pageable buffers): the kernel runs while the records
+    stream in, so nothing the host launches behind it may wait for the device
+    to go idle (a kernel's first launch loads its module).  Run in a fresh
+    child process, so that no earlier call has loaded any kernel."""
+    import subprocess
+    import sys
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    count, n = 1 << 19, 12
+    recs = P.uniform_maps(count, n, 0xF1257)
+    np.save(tmp_path / "recs.npy", recs)
+    pkg = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                       "gpgpu-binary-automaton-synchronizing-algorithms_b200")
+    code = ("import sys, numpy as np; sys.path.insert(0, sys.argv[1]); import sbfs; "
+            "r = np.load(sys.argv[2]); e = sbfs.Engine(device=0); out = e.solve(r, n=12); "
+            "np.save(sys.argv[3], out['len']); np.save(sys.argv[4], out['words'])")
+    res = subprocess.run([sys.executable, "-c", code, pkg, str(tmp_path / "recs.npy"), str(tmp_path / "len.npy"),
+                          str(tmp_path / "words.npy")], capture_output=True, text=True, timeout=600)
+    assert res.returncode == 0, res.stderr[-3000:]
+    lens = np.load(tmp_path / "len.npy")
+    words = np.load(tmp_path / "words.npy")
+    ref = oracle_mod.solve(recs, n=n, words=False, threads=8)
+    np.testing.assert_array_equal(lens, ref["len"])
+    assert oracle_mod.replay(recs, lens, words, n=n)[0] == 0
