@@ -470,6 +470,25 @@ def run_sbfs(args):
                               "p99": sorted(e2e_ms)[min(len(e2e_ms) - 1, int(0.99 * len(e2e_ms)))]}}
         if not np.array_equal(r["len"], lens):
             raise SystemExit("host and device paths disagree")
+        # the same call with pageable (numpy) buffers: records and results pass
+        # through pinned staging that host threads copy chunk by chunk
+        g_len = np.empty(count, dtype=np.int32)
+        g_words = np.empty((count, ws), dtype=np.uint64)
+        g_ns = None if wl["ns"] is None else np.ascontiguousarray(wl["ns"])
+        for i in range(min(args.warmup, 2)):
+            eng.solve(wl["recs"], ns=g_ns, n=wl["n"], lstride=lstride, word_stride=ws, out=(g_len, g_words))
+        pg_ms = []
+        for i in range(min(args.steps, 10)):
+            flush.fill_(i + 11)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            eng.solve(wl["recs"], ns=g_ns, n=wl["n"], lstride=lstride, word_stride=ws, out=(g_len, g_words))
+            pg_ms.append((time.perf_counter() - t0) * 1e3)
+        if not np.array_equal(g_len, lens):
+            raise SystemExit("pageable and device paths disagree")
+        pg_mean = max_over_ranks(dist, statistics.mean(pg_ms), dev)
+        e2e["pageable"] = {"value": count * world / (pg_mean / 1e3), "unit": UNIT, "ms_per_step": pg_mean,
+                           "steps": len(pg_ms), "buffers": "pageable numpy arrays (staged through pinned memory)"}
 
     # ---- plain form (one automaton per launch) on a sample ------------------
     plain = None

@@ -542,10 +542,12 @@ sbfs_status finish_lane(sbfs_handle *h, Lane &L, Totals &t)
     if (cudaEventElapsedTime(&ms, L.ev_k0, L.ev_k1) == cudaSuccess) t.kernel_ms += ms;
     cudaGetLastError();
     if (L.staged_out) {
-        if (L.user_len) std::memcpy(L.user_len + L.begin, L.h_len.ptr, (size_t)L.count * sizeof(int32_t));
+        CopyPool::Group g;
+        if (L.user_len) h->copy_pool().copy(L.user_len + L.begin, L.h_len.ptr, (size_t)L.count * sizeof(int32_t), g);
         if (L.user_words)
-            std::memcpy(L.user_words + (size_t)L.begin * L.word_stride, L.h_words.ptr,
-                        (size_t)L.count * L.word_stride * sizeof(uint64_t));
+            h->copy_pool().copy(L.user_words + (size_t)L.begin * L.word_stride, L.h_words.ptr,
+                                (size_t)L.count * L.word_stride * sizeof(uint64_t), g);
+        h->copy_pool().wait(g);
     }
     return SBFS_OK;
 }
@@ -674,8 +676,14 @@ sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstr
     const uint8_t *src = maps;
     if (!pin_in) {
         CK(L.h_maps.reserve(cnt * rec), "allocating pinned staging");
-        std::memcpy(L.h_maps.ptr, maps, cnt * rec);
         src = L.h_maps.as<uint8_t>();
+    }
+    if (!pin_out && (int64_t)S.ev_out.size() < nch) {
+        for (int64_t i = (int64_t)S.ev_out.size(); i < nch; ++i) {
+            cudaEvent_t e = nullptr;
+            CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "creating events");
+            S.ev_out.push_back(e);
+        }
     }
     int32_t *dst_len = out_len;
     uint64_t *dst_words = out_words;
@@ -695,6 +703,12 @@ sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstr
        "clearing chunk flags");
     auto copy_chunk_in = [&](int64_t ci) -> sbfs_status {
         const int64_t a = ci * kStreamChunk, m = std::min(kStreamChunk, cnt - a);
+        if (!pin_in) {
+            // pageable records: this chunk into pinned staging first (host threads)
+            CopyPool::Group g;
+            h->copy_pool().copy(L.h_maps.as<uint8_t>() + a * rec, maps + a * rec, m * rec, g);
+            h->copy_pool().wait(g);
+        }
         CK(cudaMemcpyAsync(L.maps.as<uint8_t>() + a * rec, src + a * rec, m * rec, cudaMemcpyHostToDevice,
                            h->copy_in),
            "copying records");
@@ -761,7 +775,21 @@ sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstr
             CK(cudaMemcpyAsync(dst_words + (size_t)a * ws, L.words.as<uint64_t>() + (size_t)a * ws,
                                (size_t)m * ws * sizeof(uint64_t), cudaMemcpyDeviceToHost, S.copy_out),
                "copying words");
+        if (!pin_out) CK(cudaEventRecord(S.ev_out[ci], S.copy_out), "recording event");
         return SBFS_OK;
+    };
+    // pageable results: a chunk whose copy into pinned staging has completed is
+    // copied on to the caller's buffers by the host threads, while later chunks
+    // are still on the device
+    CopyPool::Group g_out;
+    CopyPool::Scope g_out_scope{pin_out ? nullptr : &h->copy_pool(), g_out};
+    int64_t unstaged = 0;
+    auto stage_out = [&](int64_t ci) {
+        const int64_t a = ci * kStreamChunk, m = std::min(kStreamChunk, cnt - a);
+        if (out_len) h->copy_pool().copy(out_len + a, dst_len + a, m * sizeof(int32_t), g_out);
+        if (out_words)
+            h->copy_pool().copy(out_words + (size_t)a * ws, dst_words + (size_t)a * ws,
+                                (size_t)m * ws * sizeof(uint64_t), g_out);
     };
     const auto t_start = std::chrono::steady_clock::now();
     int64_t next = 0;
@@ -769,6 +797,10 @@ sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstr
         if (*(volatile unsigned int *)(hf + next)) {
             if ((st = copy_chunk_out(next))) return st;
             ++next;
+            continue;
+        }
+        if (!pin_out && unstaged < next && cudaEventQuery(S.ev_out[unstaged]) == cudaSuccess) {
+            stage_out(unstaged++);
             continue;
         }
         const cudaError_t q = cudaEventQuery(S.ev_kdone);
@@ -783,11 +815,13 @@ sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstr
         if ((st = copy_chunk_out(next))) return st;
     // escalated automata finish after their chunk may have been copied: store
     // their results into the host output from the device, behind the copies
+    // (pageable output: from the host, below, once the staged copies are done)
     int32_t *map_len = nullptr;
     uint64_t *map_words = nullptr;
-    bool mapped = true;
-    if (dst_len && cudaHostGetDevicePointer((void **)&map_len, dst_len, 0) != cudaSuccess) mapped = false;
-    if (dst_words && cudaHostGetDevicePointer((void **)&map_words, dst_words, 0) != cudaSuccess) mapped = false;
+    bool mapped = pin_out;
+    if (mapped && dst_len && cudaHostGetDevicePointer((void **)&map_len, dst_len, 0) != cudaSuccess) mapped = false;
+    if (mapped && dst_words && cudaHostGetDevicePointer((void **)&map_words, dst_words, 0) != cudaSuccess)
+        mapped = false;
     cudaGetLastError();
     const DevCounters *hc = L.h_counters.as<DevCounters>();
     const int64_t esc = (int64_t)hc->escal_count[c];
@@ -805,27 +839,27 @@ sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstr
         }
     }
     CK(cudaStreamSynchronize(S.copy_out), "copying results");
+    if (!pin_out) {
+        while (unstaged < nch) stage_out(unstaged++);
+        h->copy_pool().wait(g_out);
+    }
     if (esc > 0 && (out_len || out_words) && !mapped) {
         const EscalResult *r = S.h_escal.as<EscalResult>();
         for (int64_t i = 0; i < esc; ++i) {
             if (i + 16 < esc) {   // the stores miss the cache: keep several in flight
-                if (dst_len) __builtin_prefetch(dst_len + r[i + 16].k, 1);
-                if (dst_words) __builtin_prefetch(dst_words + (size_t)r[i + 16].k * ws, 1);
+                if (out_len) __builtin_prefetch(out_len + r[i + 16].k, 1);
+                if (out_words) __builtin_prefetch(out_words + (size_t)r[i + 16].k * ws, 1);
             }
             const int64_t k = r[i].k;
             if (k < 0 || k >= cnt) return fail(h, SBFS_ECUDA, "streamed solve: corrupt escalated result");
-            if (dst_len) dst_len[k] = r[i].len;
-            if (dst_words) {
-                uint64_t *w = dst_words + (size_t)k * ws;
+            if (out_len) out_len[k] = r[i].len;
+            if (out_words) {
+                uint64_t *w = out_words + (size_t)k * ws;
                 w[0] = r[i].word[0];
                 if (ws > 1) w[1] = r[i].word[1];
                 for (int j = 2; j < ws; ++j) w[j] = 0ull;
             }
         }
-    }
-    if (!pin_out) {
-        if (out_len) std::memcpy(out_len, dst_len, cnt * sizeof(int32_t));
-        if (out_words) std::memcpy(out_words, dst_words, (size_t)cnt * ws * sizeof(uint64_t));
     }
     o.expanded += (int64_t)(hc->expanded + L.level_expanded);
     o.escalated += esc;
@@ -887,7 +921,7 @@ sbfs_status solve_host(sbfs_handle *h, const uint8_t *maps, int32_t lstride, con
         }
         if (so.error & kErrInvalid) return fail(h, SBFS_EINVAL, "malformed automaton: a state index >= n");
         if (so.error & kErrBounds) return fail(h, SBFS_ECUDA, "a bounds check failed (checked build)");
-    if (so.error) return fail(h, SBFS_ETIMEOUT, "a device-side bounded wait ran out");
+        if (so.error) return fail(h, SBFS_ETIMEOUT, "a device-side bounded wait ran out");
         return SBFS_OK;
     }
     const int64_t chunk = plain ? std::max<int64_t>(count, 1)
@@ -913,13 +947,15 @@ sbfs_status solve_host(sbfs_handle *h, const uint8_t *maps, int32_t lstride, con
         const uint8_t *src_ns = ns ? ns + begin : nullptr;
         if (!pin_in) {
             CK(L.h_maps.reserve(cnt * rec), "allocating pinned staging");
-            std::memcpy(L.h_maps.ptr, src_maps, cnt * rec);
+            if (ns) CK(L.h_ns.reserve(cnt), "allocating pinned staging");
+            CopyPool::Group g;
+            h->copy_pool().copy(L.h_maps.ptr, src_maps, cnt * rec, g);
             src_maps = L.h_maps.as<uint8_t>();
             if (ns) {
-                CK(L.h_ns.reserve(cnt), "allocating pinned staging");
-                std::memcpy(L.h_ns.ptr, src_ns, cnt);
+                h->copy_pool().copy(L.h_ns.ptr, src_ns, cnt, g);
                 src_ns = L.h_ns.as<uint8_t>();
             }
+            h->copy_pool().wait(g);
         }
         L.staged_out = !pin_out;
         L.user_len = out_len;
@@ -1208,6 +1244,8 @@ sbfs_status sbfs_destroy(sbfs_handle *h)
         }
         if (S.ev_in0) cudaEventDestroy(S.ev_in0);
         if (S.ev_kdone) cudaEventDestroy(S.ev_kdone);
+        for (cudaEvent_t e : S.ev_out) cudaEventDestroy(e);
+        S.ev_out.clear();
         S.flags.release();
         S.escal_out.release();
         S.h_flags.release();

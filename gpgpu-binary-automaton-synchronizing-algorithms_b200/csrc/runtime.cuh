@@ -4,6 +4,7 @@
 
 #include <cstdint>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <set>
 #include <string>
@@ -13,6 +14,7 @@
 
 #include "classes.cuh"
 #include "common.cuh"
+#include "copy_pool.hpp"
 #include "level.cuh"
 #include "sbfs.h"
 
@@ -68,6 +70,7 @@ struct Streamer {
     DevBuf escal_out;    // EscalResult per escalation slot
     HostBuf h_flags;     // host_flag[nch] | zeros[nch] | ones[nch] (mapped)
     HostBuf h_escal;     // escal_out copied back
+    std::vector<cudaEvent_t> ev_out;   // chunk c's results are in pinned staging (pageable callers)
 };
 
 // Parameters of the one-automaton-per-lane kernel (classes 0 and 1).
@@ -193,4 +196,11 @@ struct sbfs_handle {
     // at sbfs_create): the next streamed call never sets chunk c's ready flag,
     // so the kernel's bounded wait for it runs out; then the hook is cleared
     int64_t skip_ready_chunk = -1;
+    // host threads for the staging copies of pageable callers (created on first use)
+    std::unique_ptr<sbfs::CopyPool> pool;
+    sbfs::CopyPool &copy_pool()
+    {
+        if (!pool) pool.reset(new sbfs::CopyPool(sbfs::CopyPool::default_workers()));
+        return *pool;
+    }
 };

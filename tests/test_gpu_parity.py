@@ -300,6 +300,18 @@ def test_streamed_host_path(oracle_mod, n, count):
         p = eng.solve(pin.numpy(), n=n, lstride=n, out=(out_len.numpy(), out_words.numpy().view(np.uint64)))
         np.testing.assert_array_equal(p["len"], ref["len"])
         assert oracle_mod.replay(recs, p["len"], p["words"], n=n, lstride=n)[0] == 0
+        # one side pinned, the other pageable: pageable results are staged chunk by
+        # chunk and the escalated automata's results written by the host
+        q = eng.solve(pin.numpy(), n=n, lstride=n)
+        np.testing.assert_array_equal(q["len"], ref["len"])
+        assert oracle_mod.replay(recs, q["len"], q["words"], n=n, lstride=n)[0] == 0
+        if n >= 11:
+            assert q["stats"]["escalated"] > 0
+        out_len.zero_()
+        out_words.zero_()
+        q = eng.solve(recs, n=n, lstride=n, out=(out_len.numpy(), out_words.numpy().view(np.uint64)))
+        np.testing.assert_array_equal(q["len"], ref["len"])
+        assert oracle_mod.replay(recs, q["len"], q["words"], n=n, lstride=n)[0] == 0
         v = eng.verify(recs, n=n, lstride=n)
         np.testing.assert_array_equal(v["len"], ref["len"])
         assert eng.verify(recs, n=n, lstride=n, lengths=False)["first_violation"] == -1
