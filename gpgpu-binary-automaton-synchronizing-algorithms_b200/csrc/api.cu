@@ -13,6 +13,7 @@
 //   * caller buffers in pinned memory are copied directly; pageable ones go
 //     through the lane's pinned staging buffers.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <climits>
 #include <cstdio>
@@ -629,6 +630,7 @@ std::string graph_key(const void *a, const void *b, const void *c, const void *d
 //    written to a compact array (by escalation slot), copied back at the end
 //    and patched into the host results.
 constexpr int64_t kStreamChunk = 1 << 17;   // x 2n bytes: whole 128-byte lines
+constexpr int64_t kStreamFirst = 1 << 14;   // chunk 0: the kernel starts after a short copy
 constexpr int64_t kStreamJob = 1 << 24;     // automata per kernel launch
 
 bool stream_eligible(sbfs_handle *h, const uint8_t *ns, int32_t n_uniform, int64_t count, bool plain)
@@ -652,7 +654,10 @@ sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstr
     Lane &L = h->lanes[0];
     Streamer &S = h->streamer;
     const size_t rec = 2 * (size_t)lstride;
-    const int64_t nch = (cnt + kStreamChunk - 1) / kStreamChunk;
+    LaneStream geo{};
+    geo.chunk = kStreamChunk;
+    geo.first = kStreamFirst;
+    const int64_t nch = geo.chunks(cnt);
     const int c = class_of_n(n);
     const LaneShape &ls = h->plan.lane[c];
     CK(L.maps.reserve(cnt * rec), "allocating records");
@@ -702,7 +707,7 @@ sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstr
     CK(cudaMemcpyAsync(ready, hf + nch, nch * sizeof(unsigned int), cudaMemcpyHostToDevice, h->copy_in),
        "clearing chunk flags");
     auto copy_chunk_in = [&](int64_t ci) -> sbfs_status {
-        const int64_t a = ci * kStreamChunk, m = std::min(kStreamChunk, cnt - a);
+        const int64_t a = geo.chunk_begin(ci), m = geo.chunk_size(ci, cnt);
         if (!pin_in) {
             // pageable records: this chunk into pinned staging first (host threads)
             CopyPool::Group g;
@@ -741,8 +746,12 @@ sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstr
     b.first_violation = &ctr->first_violation;
     b.expanded = &ctr->expanded;
     b.error = &ctr->error;
-    LaneStream lsd{ready, done, d_host_flag, kStreamChunk, S.escal_out.as<EscalResult>(),
-                   h->cfg.wait_polls > 0 ? h->cfg.wait_polls : (1 << 24)};
+    LaneStream lsd = geo;
+    lsd.chunk_ready = ready;
+    lsd.chunk_done = done;
+    lsd.host_flag = d_host_flag;
+    lsd.escal_out = S.escal_out.as<EscalResult>();
+    lsd.wait_polls = h->cfg.wait_polls > 0 ? h->cfg.wait_polls : (1 << 24);
     CK(cudaEventRecord(L.ev_k0, L.stream), "recording event");
     CK(launch_lane(ls.nmax, ls.warps, ls.ring, ls.refill_k, ls.tail_k, ls.ctas, b, L.escal.as<int32_t>(),
                    (unsigned long long)cnt, &ctr->escal_count[c], &ctr->escal_claim[c], &ctr->ticket[c], lsd,
@@ -766,7 +775,7 @@ sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstr
     CK(cudaEventRecord(S.ev_kdone, L.stream), "recording event");
     // results out, chunk by chunk, as the kernel finishes them
     auto copy_chunk_out = [&](int64_t ci) -> sbfs_status {
-        const int64_t a = ci * kStreamChunk, m = std::min(kStreamChunk, cnt - a);
+        const int64_t a = geo.chunk_begin(ci), m = geo.chunk_size(ci, cnt);
         if (out_len)
             CK(cudaMemcpyAsync(dst_len + a, L.len.as<int32_t>() + a, m * sizeof(int32_t), cudaMemcpyDeviceToHost,
                                S.copy_out),
@@ -785,7 +794,7 @@ sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstr
     CopyPool::Scope g_out_scope{pin_out ? nullptr : &h->copy_pool(), g_out};
     int64_t unstaged = 0;
     auto stage_out = [&](int64_t ci) {
-        const int64_t a = ci * kStreamChunk, m = std::min(kStreamChunk, cnt - a);
+        const int64_t a = geo.chunk_begin(ci), m = geo.chunk_size(ci, cnt);
         if (out_len) h->copy_pool().copy(out_len + a, dst_len + a, m * sizeof(int32_t), g_out);
         if (out_words)
             h->copy_pool().copy(out_words + (size_t)a * ws, dst_words + (size_t)a * ws,
@@ -844,22 +853,30 @@ sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstr
         h->copy_pool().wait(g_out);
     }
     if (esc > 0 && (out_len || out_words) && !mapped) {
+        // random stores into the caller's buffers, spread over the host threads
         const EscalResult *r = S.h_escal.as<EscalResult>();
-        for (int64_t i = 0; i < esc; ++i) {
-            if (i + 16 < esc) {   // the stores miss the cache: keep several in flight
-                if (out_len) __builtin_prefetch(out_len + r[i + 16].k, 1);
-                if (out_words) __builtin_prefetch(out_words + (size_t)r[i + 16].k * ws, 1);
+        std::atomic<bool> corrupt{false};
+        h->copy_pool().parallel_for((size_t)esc, 2048, [&](size_t i0, size_t i1) {
+            for (size_t i = i0; i < i1; ++i) {
+                if (i + 16 < i1) {   // the stores miss the cache: keep several in flight
+                    if (out_len) __builtin_prefetch(out_len + r[i + 16].k, 1);
+                    if (out_words) __builtin_prefetch(out_words + (size_t)r[i + 16].k * ws, 1);
+                }
+                const int64_t k = r[i].k;
+                if (k < 0 || k >= cnt) {
+                    corrupt.store(true, std::memory_order_relaxed);
+                    continue;
+                }
+                if (out_len) out_len[k] = r[i].len;
+                if (out_words) {
+                    uint64_t *w = out_words + (size_t)k * ws;
+                    w[0] = r[i].word[0];
+                    if (ws > 1) w[1] = r[i].word[1];
+                    for (int j = 2; j < ws; ++j) w[j] = 0ull;
+                }
             }
-            const int64_t k = r[i].k;
-            if (k < 0 || k >= cnt) return fail(h, SBFS_ECUDA, "streamed solve: corrupt escalated result");
-            if (out_len) out_len[k] = r[i].len;
-            if (out_words) {
-                uint64_t *w = out_words + (size_t)k * ws;
-                w[0] = r[i].word[0];
-                if (ws > 1) w[1] = r[i].word[1];
-                for (int j = 2; j < ws; ++j) w[j] = 0ull;
-            }
-        }
+        });
+        if (corrupt.load()) return fail(h, SBFS_ECUDA, "streamed solve: corrupt escalated result");
     }
     o.expanded += (int64_t)(hc->expanded + L.level_expanded);
     o.escalated += esc;

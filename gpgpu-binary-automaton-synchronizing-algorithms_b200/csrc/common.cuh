@@ -145,9 +145,25 @@ struct LaneStream {
     const unsigned int *chunk_ready;   // nonzero once chunk c's records are on the device
     unsigned int *chunk_done;          // lane outcomes recorded per chunk (starts at 0)
     unsigned int *host_flag;           // mapped host memory: 1 once chunk c's outcomes are all written
-    int64_t chunk;                     // automata per chunk (records of a chunk fill whole 128-byte lines)
+    int64_t chunk;                     // automata per chunk after the first (whole 128-byte lines of records)
     EscalResult *escal_out;            // by escalation slot: results the whole-warp search writes
     int wait_polls;                    // bounded wait for a chunk's records: polls before giving up
+    // automata in chunk 0, at most `chunk`: a short first copy lets the kernel
+    // start sooner (whole 128-byte lines of records too)
+    int64_t first;
+
+    __host__ __device__ int64_t chunk_of(int64_t k) const { return k < first ? 0 : 1 + (k - first) / chunk; }
+    __host__ __device__ int64_t chunk_begin(int64_t c) const { return c == 0 ? 0 : first + (c - 1) * chunk; }
+    // chunks of a batch of `count` automata, and the size of chunk c
+    __host__ __device__ int64_t chunks(int64_t count) const
+    {
+        return count <= first ? 1 : 1 + (count - first + chunk - 1) / chunk;
+    }
+    __host__ __device__ int64_t chunk_size(int64_t c, int64_t count) const
+    {
+        const int64_t a = chunk_begin(c), e = chunk_begin(c + 1);
+        return (e < count ? e : count) - a;
+    }
 };
 
 // Stores the first *count escalated results into device-accessible (e.g.

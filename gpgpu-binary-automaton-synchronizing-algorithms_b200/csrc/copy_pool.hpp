@@ -18,6 +18,7 @@
 #include <deque>
 #include <mutex>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 namespace sbfs {
@@ -74,11 +75,47 @@ public:
             size_t a = 0;
             for (size_t p = 0; p < parts; ++p) {
                 const size_t len = p + 1 == parts ? n - a : std::min(per, n - a);
-                tasks_.push_back(Task{static_cast<char *>(dst) + a, static_cast<const char *>(src) + a, len, &g});
+                Task t;
+                t.dst = static_cast<char *>(dst) + a;
+                t.src = static_cast<const char *>(src) + a;
+                t.n = len;
+                t.g = &g;
+                tasks_.push_back(t);
                 a += len;
             }
         }
         cv_.notify_all();
+    }
+
+    // Runs f(begin, end) over [0, n) in parts of at least `grain` items, on the
+    // workers and this thread; returns when every part is done.
+    template <class F>
+    void parallel_for(size_t n, size_t grain, F &&f)
+    {
+        if (n == 0) return;
+        const size_t parts = std::max<size_t>(1, std::min(threads_.size() + 1, n / std::max<size_t>(grain, 1)));
+        if (parts == 1) {
+            f(size_t(0), n);
+            return;
+        }
+        using Fn = typename std::remove_reference<F>::type;
+        void (*call)(void *, size_t, size_t) = [](void *ctx, size_t a, size_t b) { (*static_cast<Fn *>(ctx))(a, b); };
+        Group g;
+        g.left.store((long)parts, std::memory_order_relaxed);
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            for (size_t p = 0; p < parts; ++p) {
+                Task t;
+                t.call = call;
+                t.ctx = const_cast<void *>(static_cast<const void *>(&f));
+                t.a = n * p / parts;
+                t.b = n * (p + 1) / parts;
+                t.g = &g;
+                tasks_.push_back(t);
+            }
+        }
+        cv_.notify_all();
+        wait(g);
     }
 
     // Waits for a group when it goes out of scope, early returns included, so
@@ -108,16 +145,23 @@ public:
 private:
     static constexpr size_t kMinSlice = 256u << 10;
 
+    // a slice of a copy, or (call set) a part [a, b) of a parallel_for
     struct Task {
         char *dst = nullptr;
         const char *src = nullptr;
         size_t n = 0;
         Group *g = nullptr;
+        void (*call)(void *, size_t, size_t) = nullptr;
+        void *ctx = nullptr;
+        size_t a = 0, b = 0;
     };
 
     static void run(const Task &t)
     {
-        std::memcpy(t.dst, t.src, t.n);
+        if (t.call)
+            t.call(t.ctx, t.a, t.b);
+        else
+            std::memcpy(t.dst, t.src, t.n);
         t.g->left.fetch_sub(1, std::memory_order_acq_rel);
     }
 

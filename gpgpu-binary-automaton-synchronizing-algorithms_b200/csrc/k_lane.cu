@@ -302,12 +302,12 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
                 const unsigned om = __ballot_sync(kFull, outcome);
                 if (outcome) {
                     __threadfence();   // this lane's results before its count
-                    const int64_t c = k / ls.chunk;
+                    const int64_t c = ls.chunk_of(k);
                     const unsigned grp = __match_any_sync(om, (unsigned long long)c);
                     if (lane == __ffs(grp) - 1) {
                         const unsigned add = (unsigned)__popc(grp);
                         const unsigned old = atomicAdd(ls.chunk_done + c, add);
-                        const int64_t size = min(ls.chunk, count - c * ls.chunk);
+                        const int64_t size = ls.chunk_size(c, count);
                         if ((int64_t)(old + add) == size) {
                             __threadfence_system();
                             *(volatile unsigned int *)(ls.host_flag + c) = 1u;
@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
                     // streamed batch: the records handed out must have arrived
                     const int64_t last = (int64_t)min(got + (unsigned long long)__popc(idle),
                                                       (unsigned long long)count) - 1;
-                    const int64_t c_last = last / ls.chunk;
+                    const int64_t c_last = ls.chunk_of(last);
                     if (c_last > ready_upto) {
                         bool ok = true;
                         if (lane == 0) ok = wait_chunk(ls.chunk_ready, c_last, ls.wait_polls);
@@ -609,7 +609,8 @@ cudaError_t launch_lane(int nmax, int warps, int ring, int refill_k, int tail_k,
     if ((ring & (ring - 1)) || ring < 8 || warps < 1 || warps > 8 || ctas < 1 || refill_k < 1 || refill_k > 32 ||
         tail_k < 0 || tail_k > 32)
         return cudaErrorInvalidValue;
-    if (ls.chunk_done && (ls.chunk < 1 || b.order || b.range_dev)) return cudaErrorInvalidValue;
+    if (ls.chunk_done && (ls.chunk < 1 || ls.first < 1 || ls.first > ls.chunk || b.order || b.range_dev))
+        return cudaErrorInvalidValue;
     const bool words = b.out_words != nullptr;
     if (nmax <= 8)
         return words ? launch_t<8, true>(warps, ring, refill_k, tail_k, ctas, b, escal_list, escal_capacity,

@@ -3,7 +3,8 @@
 Compiled with g++ into a small driver and run on the CPU: copies of many sizes
 and misaligned offsets, several groups in flight at once, a group waited for by
 its scope guard, and worker counts from none to eight must each give a byte-exact
-copy and leave no slice running after wait() returns."""
+copy and leave no slice running after wait() returns; parallel_for must visit
+every index exactly once."""
 import os
 import subprocess
 
@@ -60,6 +61,12 @@ int main() {
             pool.copy(d2.data(), s2.data(), s2.size(), g2);
         }
         bad += check(s2, d2, 0, s2.size());
+        // parallel_for visits every index exactly once, in disjoint parts
+        for (size_t n : {size_t(0), size_t(1), size_t(100), size_t(12345), size_t(1) << 20}) {
+            std::vector<int> hit(n, 0);
+            pool.parallel_for(n, 1000, [&](size_t a, size_t b) { for (size_t i = a; i < b; ++i) hit[i] += 1; });
+            for (size_t i = 0; i < n; ++i) bad += hit[i] != 1;
+        }
     }
     std::printf("default_workers=%d bad=%d\n", CopyPool::default_workers(), bad);
     return bad ? 1 : 0;
