@@ -466,7 +466,7 @@ def test_bounded_device_wait_runs_out_and_the_handle_recovers(oracle_mod):
     recs = P.repack(P.uniform_maps(count, n, 0xB0B), 32, n)
     os.environ["SBFS_TEST_SKIP_CHUNK_READY"] = "2"
     try:
-        eng = sbfs.Engine(device=0, wait_polls=1 << 10)
+        eng = sbfs.Engine(device=0, wait_polls=1 << 12)   # about 1 ms of polls
     finally:
         del os.environ["SBFS_TEST_SKIP_CHUNK_READY"]
     with eng:
