@@ -333,10 +333,15 @@ def test_streamed_path_violation_and_malformed(oracle_mod):
         assert v["first_violation"] == 333_333 and v["len"][333_333] == 121
     bad = recs.copy()
     bad[299_999, 3] = 12   # state 12 in a 12-state automaton
+    bad[123_456, 20] = 200   # b(8) = 200: far out of range
+    out_len = np.zeros(count, dtype=np.int32)
+    out_words = np.zeros((count, 2), dtype=np.uint64)
     with sbfs.Engine(device=0) as eng:
         with pytest.raises(sbfs.SbfsError) as ei:
-            eng.solve(bad, n=12, lstride=12)
+            eng.solve(bad, n=12, lstride=12, out=(out_len, out_words))
         assert ei.value.status == 1
+        assert out_len[299_999] == -2 and out_len[123_456] == -2
+        assert (out_len >= -1).sum() == count - 2
         r = eng.solve(recs, n=12, lstride=12)   # the handle stays usable
         assert r["first_violation"] == -1 and r["len"][333_333] == 121
 
