@@ -30,9 +30,14 @@ public:
         std::atomic<long> left{0};
     };
 
+    // Starts up to `workers` threads; fewer if the system refuses more (the
+    // waiting thread does the rest of the work, so none is needed).
     explicit CopyPool(int workers)
     {
-        for (int i = 0; i < workers; ++i) threads_.emplace_back([this] { loop(); });
+        try {
+            for (int i = 0; i < workers; ++i) threads_.emplace_back([this] { loop(); });
+        } catch (...) {
+        }
     }
 
     ~CopyPool()
@@ -67,13 +72,13 @@ public:
             std::memcpy(dst, src, n);
             return;
         }
-        // slices on 64-byte boundaries (cache lines), the last one takes the rest
+        // slices on 64-byte boundaries (cache lines), the last one takes the rest;
+        // a slice that cannot be queued (no memory) is copied here instead
         const size_t per = ((n / parts) + 63) & ~size_t(63);
-        g.left.fetch_add((long)parts, std::memory_order_relaxed);
-        {
+        size_t a = 0;
+        try {
             std::lock_guard<std::mutex> lk(mu_);
-            size_t a = 0;
-            for (size_t p = 0; p < parts; ++p) {
+            for (size_t p = 0; p < parts && a < n; ++p) {
                 const size_t len = p + 1 == parts ? n - a : std::min(per, n - a);
                 Task t;
                 t.dst = static_cast<char *>(dst) + a;
@@ -81,10 +86,13 @@ public:
                 t.n = len;
                 t.g = &g;
                 tasks_.push_back(t);
+                g.left.fetch_add(1, std::memory_order_relaxed);
                 a += len;
             }
+        } catch (...) {
         }
         cv_.notify_all();
+        if (a < n) std::memcpy(static_cast<char *>(dst) + a, static_cast<const char *>(src) + a, n - a);
     }
 
     // Runs f(begin, end) over [0, n) in parts of at least `grain` items, on the
@@ -101,10 +109,10 @@ public:
         using Fn = typename std::remove_reference<F>::type;
         void (*call)(void *, size_t, size_t) = [](void *ctx, size_t a, size_t b) { (*static_cast<Fn *>(ctx))(a, b); };
         Group g;
-        g.left.store((long)parts, std::memory_order_relaxed);
-        {
+        size_t p = 0;
+        try {
             std::lock_guard<std::mutex> lk(mu_);
-            for (size_t p = 0; p < parts; ++p) {
+            for (; p < parts; ++p) {
                 Task t;
                 t.call = call;
                 t.ctx = const_cast<void *>(static_cast<const void *>(&f));
@@ -112,9 +120,12 @@ public:
                 t.b = n * (p + 1) / parts;
                 t.g = &g;
                 tasks_.push_back(t);
+                g.left.fetch_add(1, std::memory_order_relaxed);
             }
+        } catch (...) {
         }
         cv_.notify_all();
+        if (p < parts) f(n * p / parts, n);   // parts that could not be queued
         wait(g);
     }
 

@@ -6,6 +6,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <new>
 #include <set>
 #include <string>
 #include <vector>
@@ -200,7 +201,11 @@ struct sbfs_handle {
     std::unique_ptr<sbfs::CopyPool> pool;
     sbfs::CopyPool &copy_pool()
     {
-        if (!pool) pool.reset(new sbfs::CopyPool(sbfs::CopyPool::default_workers()));
+        if (!pool) pool.reset(new (std::nothrow) sbfs::CopyPool(sbfs::CopyPool::default_workers()));
+        if (!pool) {
+            static sbfs::CopyPool inline_only(0);   // no memory for a pool: copy on the calling thread
+            return inline_only;
+        }
         return *pool;
     }
 };
