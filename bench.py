@@ -44,6 +44,7 @@ import socket
 import statistics
 import subprocess
 import sys
+import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -180,6 +181,62 @@ def word_stride_for(max_n: int) -> int:
 # ---------------------------------------------------------------------------
 # clocks during the timed region
 # ---------------------------------------------------------------------------
+
+class NvmlClockSampler:
+    """SM clock and clock-event reasons read through NVML every `period` seconds
+    on a background thread while the timed steps run (reads only: nothing about
+    the GPU is set).  The timed region of the default workload lasts ~12 ms,
+    shorter than nvidia-smi takes to start, so polling NVML is what places the
+    samples inside it."""
+
+    def __init__(self, gpu_index: int, period: float = 0.0005):
+        import pynvml
+        self.nv = pynvml
+        pynvml.nvmlInit()
+        self.h = pynvml.nvmlDeviceGetHandleByIndex(gpu_index)
+        self.max = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        self.period = period
+        self.samples = []
+        self.done = threading.Event()
+        self.thread = threading.Thread(target=self._run, daemon=True)
+        self.thread.start()
+
+    def _run(self):
+        nv = self.nv
+        while True:
+            try:
+                self.samples.append((nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM),
+                                     nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)))
+            except nv.NVMLError:
+                pass
+            if self.done.wait(self.period):
+                return
+
+    def stop(self):
+        self.done.set()
+        self.thread.join()
+        nv = self.nv
+        try:
+            nv.nvmlShutdown()
+        except nv.NVMLError:
+            pass
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        reasons = sorted({name for _, r in self.samples for name, b in bits.items() if r & b})
+        sm = [s for s, _ in self.samples]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": float(self.max),
+                "reasons": reasons, "samples": len(sm), "source": "NVML, polled during the timed steps"}
+
+
+def clock_sampler(gpu_index: int):
+    """NVML polling when the bindings load, else nvidia-smi."""
+    try:
+        return NvmlClockSampler(gpu_index)
+    except Exception:
+        return ClockSampler(gpu_index)
+
 
 class ClockSampler:
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -430,7 +487,7 @@ def run_sbfs(args):
     visible = [v for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip().isdigit()]
     gpu_index = int(visible[dev.index]) if dev.index < len(visible) else dev.index
     step_ms, stats, clk = leg.timed(args.steps, args.warmup, flush, barrier,
-                                    (lambda: ClockSampler(gpu_index)) if rank == 0 else None)
+                                    (lambda: clock_sampler(gpu_index)) if rank == 0 else None)
     ms = statistics.mean(step_ms)
     ms_max = max_over_ranks(dist, ms, dev)
     value = count * world / (ms_max / 1e3)
