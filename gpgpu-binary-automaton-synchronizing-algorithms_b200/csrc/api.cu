@@ -627,8 +627,12 @@ std::string graph_key(const void *a, const void *b, const void *c, const void *d
 //  - this thread polls those flags and copies each finished chunk's lengths
 //    and words out on copy_out while the kernel still runs;
 //  - automata solved by the whole-warp search finish late: they are also
-//    written to a compact array (by escalation slot), copied back at the end
-//    and patched into the host results.
+//    written to a compact array (by escalation slot) and, after the last
+//    chunk's copy, stored into the host results by a small kernel through
+//    mapped memory (pinned results) or by the host threads (pageable ones);
+//  - a pageable caller's records are staged into pinned memory chunk by
+//    chunk, and its results go on from pinned staging as each chunk lands,
+//    both by the handle's host copy threads.
 constexpr int64_t kStreamChunk = 1 << 17;   // x 2n bytes: whole 128-byte lines
 // Chunk 0's size.  A 2^14-automaton first chunk (the kernel starts after a
 // 0.4 MB copy instead of 3 MB) measured the same end to end with pinned buffers
