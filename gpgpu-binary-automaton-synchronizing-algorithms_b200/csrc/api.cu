@@ -244,6 +244,12 @@ sbfs_status run_level_class(sbfs_handle *h, Lane &L, const Job &j, const Batch &
     return SBFS_OK;
 }
 
+// A uniform batch of n = 13 runs on the per-lane kernel k_lane<13>.
+bool lane13_batch(const sbfs_handle *h, const uint8_t *ns, int32_t n_uniform)
+{
+    return h->plan.use_lane13 && !ns && n_uniform == 13;
+}
+
 // Reserve the lane's work buffers for a job and enqueue its kernels on the lane's
 // stream.  Counters must already be reset.
 sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches, bool plain = false,
@@ -297,14 +303,17 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
             CK(cudaStreamWaitEvent(cs, L.ev_fork, 0), "ordering streams");
             joined[c] = true;
         }
-        if (c < 2 && !plain && !P.use_pool[c]) {
-            const LaneShape &ls = P.lane[c];
-            // one escalation list per lane class; entries read as -1 until stored
+        const bool lane13 = c == 2 && !plain && !ticket_override && lane13_batch(h, j.ns, j.n_uniform);
+        if ((c < 2 && !plain && !P.use_pool[c]) || lane13) {
+            const LaneShape &ls = lane13 ? P.lane13 : P.lane[c];
+            // one escalation list per lane class (a uniform n = 13 batch has no
+            // class 1 and takes its list and counters); entries read as -1 until stored
+            const int lc = lane13 ? 1 : c;
             CK(L.escal.reserve(2 * escal_entries * sizeof(int32_t)), "allocating escalation list");
-            int32_t *list = L.escal.as<int32_t>() + (size_t)c * escal_entries;
+            int32_t *list = L.escal.as<int32_t>() + (size_t)lc * escal_entries;
             CK(cudaMemsetAsync(list, 0xFF, escal_entries * sizeof(int32_t), cs), "resetting escalation list");
             CK(launch_lane(ls.nmax, ls.warps, ls.ring, ls.refill_k, ls.tail_k, ls.ctas, bc, list, escal_entries,
-                           &ctr->escal_count[c], &ctr->escal_claim[c], ticket, LaneStream{}, cs),
+                           &ctr->escal_count[lc], &ctr->escal_claim[lc], ticket, LaneStream{}, cs),
                "launching per-lane kernel");
         } else if ((c == 2 && P.class2_hash && !plain && !ticket_override) ||
                    (c == 3 && P.class3_hash && !P.class3_level)) {
@@ -466,6 +475,18 @@ sbfs_status ensure_plan(sbfs_handle *h)
         const int per_sm = lane_max_ctas_per_sm(ls.nmax, ls.warps, ls.ring);
         if (per_sm < 1) return fail(h, SBFS_EINVAL, "per-lane kernel shape does not fit in shared memory");
         ls.ctas = per_sm * sms;
+    }
+    {
+        // uniform n = 13: 1 KB of bitmap per lane; ring 32 keeps five one-warp CTAs per SM
+        LaneShape &ls = P.lane13;
+        ls.nmax = 13;
+        ls.warps = 1;
+        ls.ring = 32;
+        ls.refill_k = 16;
+        ls.tail_k = 4;
+        const int per_sm = lane_max_ctas_per_sm(13, ls.warps, ls.ring);
+        ls.ctas = per_sm * sms;
+        P.use_lane13 = per_sm > 0 && h->cfg.small_kernel != 2 ? 1 : 0;
     }
     P.cta.threads = 1024;   // the autotuner's pick with Cerny members in the batch
     P.cta.ctas = sms * 4;
@@ -646,7 +667,7 @@ bool stream_eligible(sbfs_handle *h, const uint8_t *ns, int32_t n_uniform, int64
 {
     if (plain || ns || h->cfg.chunk != 0 || count < 2 * kStreamChunk) return false;
     const int c = class_of_n(n_uniform);
-    return c < 2 && !h->plan.use_pool[c];
+    return (c < 2 && !h->plan.use_pool[c]) || lane13_batch(h, ns, n_uniform);
 }
 
 struct StreamOut {
@@ -668,7 +689,9 @@ sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstr
     geo.first = kStreamFirst;
     const int64_t nch = geo.chunks(cnt);
     const int c = class_of_n(n);
-    const LaneShape &ls = h->plan.lane[c];
+    // n = 13 (class 2) runs on k_lane<13> with class 1's escalation counters
+    const int lc = c < 2 ? c : 1;
+    const LaneShape &ls = c < 2 ? h->plan.lane[c] : h->plan.lane13;
     CK(L.maps.reserve(cnt * rec), "allocating records");
     if (out_len) CK(L.len.reserve(cnt * sizeof(int32_t)), "allocating lengths");
     if (out_words) CK(L.words.reserve((size_t)cnt * ws * sizeof(uint64_t)), "allocating words");
@@ -763,7 +786,7 @@ sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstr
     lsd.wait_polls = h->cfg.wait_polls > 0 ? h->cfg.wait_polls : (1 << 24);
     CK(cudaEventRecord(L.ev_k0, L.stream), "recording event");
     CK(launch_lane(ls.nmax, ls.warps, ls.ring, ls.refill_k, ls.tail_k, ls.ctas, b, L.escal.as<int32_t>(),
-                   (unsigned long long)cnt, &ctr->escal_count[c], &ctr->escal_claim[c], &ctr->ticket[c], lsd,
+                   (unsigned long long)cnt, &ctr->escal_count[lc], &ctr->escal_claim[lc], &ctr->ticket[c], lsd,
                    L.stream),
        "launching per-lane kernel");
     CK(cudaEventRecord(L.ev_k1, L.stream), "recording event");
@@ -856,10 +879,10 @@ sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstr
         mapped = false;
     cudaGetLastError();
     const DevCounters *hc = L.h_counters.as<DevCounters>();
-    const int64_t esc = (int64_t)hc->escal_count[c];
+    const int64_t esc = (int64_t)hc->escal_count[lc];
     if (esc > 0 && (out_len || out_words)) {
         if (mapped) {
-            CK(launch_escal_patch(S.escal_out.as<EscalResult>(), &ctr->escal_count[c], map_len, map_words, ws,
+            CK(launch_escal_patch(S.escal_out.as<EscalResult>(), &ctr->escal_count[lc], map_len, map_words, ws,
                                   h->sm_count, S.copy_out),
                "launching result patch");
             o.launches += 1;
@@ -893,9 +916,7 @@ sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstr
                 if (out_len) out_len[k] = r[i].len;
                 if (out_words) {
                     uint64_t *w = out_words + (size_t)k * ws;
-                    w[0] = r[i].word[0];
-                    if (ws > 1) w[1] = r[i].word[1];
-                    for (int j = 2; j < ws; ++j) w[j] = 0ull;
+                    for (int j = 0; j < ws; ++j) w[j] = j < 3 ? r[i].word[j] : 0ull;
                 }
             }
         });
@@ -1444,7 +1465,12 @@ int32_t sbfs_describe_plan(sbfs_handle *h, char *buf, int32_t len)
     char tmp[256];
     for (int c = 0; c < 3; ++c) {
         const bool lane = c < 2 && !P.use_pool[c];
-        if (lane) {
+        if (c == 2 && P.class2_hash && P.use_lane13) {
+            std::snprintf(tmp, sizeof tmp,
+                          "{\"class\":2,\"max_n\":16,\"kernel\":\"k_hash+k_cta\",\"slots\":%d,"
+                          "\"uniform_n13\":\"k_lane<13>\",\"ring13\":%d,\"ctas13\":%d},",
+                          P.class2_hash == 2 ? 4096 : 2048, P.lane13.ring, P.lane13.ctas);
+        } else if (lane) {
             const LaneShape &l = P.lane[c];
             std::snprintf(tmp, sizeof tmp,
                           "{\"class\":%d,\"max_n\":%d,\"kernel\":\"k_lane<%d>\",\"warps\":%d,\"ring\":%d,"

@@ -139,7 +139,7 @@ struct EscalResult {
     int64_t k;          // automaton
     int32_t len;
     int32_t pad;
-    uint64_t word[2];   // n <= 12: at most 121 letters
+    uint64_t word[3];   // n <= 13: at most 144 letters
 };
 struct LaneStream {
     const unsigned int *chunk_ready;   // nonzero once chunk c's records are on the device

@@ -1,4 +1,4 @@
-// k_lane.cu -- power-set BFS with one automaton per lane (n <= 12).
+// k_lane.cu -- power-set BFS with one automaton per lane (n <= 13).
 //
 // Each lane runs the sequential BFS of GPGPU/CPU/SlimCPU4bits.cs:214-306 on its
 // own automaton: pop subsets, look up both images in its nibble table
@@ -63,6 +63,7 @@ struct LaneGeom {
     static constexpr int kTable = kChunks * 16;
     static constexpr uint32_t kMask = (1u << NMAX) - 1u;
     static constexpr int kWordMax = 32 - NMAX;   // letters an entry can carry
+    static constexpr int kWordU64 = ((NMAX - 1) * (NMAX - 1) + 63) / 64;   // words of the whole-warp search
 };
 
 template <int NMAX>
@@ -71,6 +72,7 @@ __device__ __forceinline__ uint32_t lane_image(const uint32_t *tb, uint32_t x)
     uint32_t t = tb[(x & 15u) * 32];
     if (LaneGeom<NMAX>::kChunks > 1) t |= tb[(16 + ((x >> 4) & 15u)) * 32];
     if (LaneGeom<NMAX>::kChunks > 2) t |= tb[(32 + ((x >> 8) & 15u)) * 32];
+    if (LaneGeom<NMAX>::kChunks > 3) t |= tb[(48 + ((x >> 12) & 15u)) * 32];
     return t;
 }
 
@@ -132,9 +134,9 @@ __device__ void warp_solve(const Batch &b, int64_t k, uint32_t *region, int lane
     uint32_t *q = region + BW;    // linear queue, 2^NMAX entries
     const int n = automaton_n(b, k);
     const uint8_t *rec = b.maps + (size_t)k * 2u * (size_t)b.lstride;
-    // chunks 0 and 1 in lanes 0-15 / 16-31 of t01, chunk 2 in lanes 0-15 of t2
+    // chunks 0 and 1 in lanes 0-15 / 16-31 of t01, chunks 2 and 3 likewise in t23
     const uint32_t t01 = table_entry<NMAX>(rec, b.lstride, n, lane >> 4, lane & 15);
-    const uint32_t t2 = G::kChunks > 2 ? table_entry<NMAX>(rec, b.lstride, n, 2, lane & 15) : 0u;
+    const uint32_t t23 = G::kChunks > 2 ? table_entry<NMAX>(rec, b.lstride, n, 2 + (lane >> 4), lane & 15) : 0u;
     for (int w = lane; w < BW; w += 32) bm[w] = 0u;
     __syncwarp();
     const uint32_t full = (1u << n) - 1u;
@@ -152,7 +154,8 @@ __device__ void warp_solve(const Batch &b, int64_t k, uint32_t *region, int lane
         const bool has = idx < lvl_end;
         const uint32_t x = has ? (q[idx] & G::kMask) : 0u;
         uint32_t t = __shfl_sync(kFull, t01, (int)(x & 15u)) | __shfl_sync(kFull, t01, 16 + (int)((x >> 4) & 15u));
-        if (G::kChunks > 2) t |= __shfl_sync(kFull, t2, (int)((x >> 8) & 15u));
+        if (G::kChunks > 2) t |= __shfl_sync(kFull, t23, (int)((x >> 8) & 15u));
+        if (G::kChunks > 3) t |= __shfl_sync(kFull, t23, 16 + (int)((x >> 12) & 15u));
         const uint32_t ya = t >> 16, yb = t & 0xFFFFu;
         expanded += has ? 1u : 0u;
         const bool sa = has && is_singleton(ya), sb = has && is_singleton(yb);
@@ -189,13 +192,16 @@ __device__ void warp_solve(const Batch &b, int64_t k, uint32_t *region, int lane
     }
     if (lane == 0) {
         record_result(b, k, n, len);
-        uint64_t w0 = 0, w1 = 0;
+        // at most (NMAX - 1)^2 letters: 2 words at n = 12, 3 at n = 13
+        static_assert(G::kWordU64 <= 3, "words of at most 192 letters");
+        uint64_t w0 = 0, w1 = 0, w2 = 0;
         if (WORDS) {
             // letters from the root: entry at depth d + 1 holds letter d
             if (len > 0) {
                 auto set = [&](uint32_t d) {
                     if (d < 64) w0 |= 1ull << d;
                     else if (d < 128) w1 |= 1ull << (d - 64);
+                    else if (G::kWordU64 > 2) w2 |= 1ull << (d - 128);
                 };
                 if (found_letter) set(level);
                 uint32_t i = found;
@@ -208,7 +214,8 @@ __device__ void warp_solve(const Batch &b, int64_t k, uint32_t *region, int lane
             uint64_t *w = b.out_words + (size_t)k * (size_t)b.word_stride;
             w[0] = w0;
             if (b.word_stride > 1) w[1] = w1;
-            for (int c = 2; c < b.word_stride; ++c) w[c] = 0ull;
+            if (b.word_stride > 2) w[2] = w2;
+            for (int c = 3; c < b.word_stride; ++c) w[c] = 0ull;
         }
         if (STREAM && ls.escal_out) {
             // streamed batches: the host patches escalated automata from here
@@ -218,6 +225,7 @@ __device__ void warp_solve(const Batch &b, int64_t k, uint32_t *region, int lane
             r.pad = 0;
             r.word[0] = w0;
             r.word[1] = w1;
+            r.word[2] = w2;
             ls.escal_out[slot] = r;
         }
         publish_result(b, k);
@@ -541,7 +549,8 @@ cudaError_t launch_t(int warps, int ring, int refill_k, int tail_k, int ctas, co
 {
     using G = LaneGeom<NMAX>;
     // the warp-cooperative search needs the bitmap and 2^NMAX queue entries in one region
-    static_assert(G::kTable * 32 >= G::kBitmapWords, "region too small for the warp search");
+    if ((size_t)G::kBitmapWords + ((size_t)1 << NMAX) > (size_t)(G::kBitmapWords + G::kTable + ring) * 32)
+        return cudaErrorInvalidValue;
     const size_t smem = smem_for<NMAX>(warps, ring);
     // the streamed form's bookkeeping is compiled out of the resident-batch kernel
     auto kernel = ls.chunk_done ? k_lane<NMAX, WORDS, true> : k_lane<NMAX, WORDS, false>;
@@ -556,12 +565,15 @@ cudaError_t launch_t(int warps, int ring, int refill_k, int tail_k, int ctas, co
 
 size_t lane_smem_bytes(int nmax, int warps, int ring)
 {
-    return nmax <= 8 ? smem_for<8>(warps, ring) : smem_for<12>(warps, ring);
+    return nmax <= 8 ? smem_for<8>(warps, ring) : nmax <= 12 ? smem_for<12>(warps, ring) : smem_for<13>(warps, ring);
 }
 
 int lane_max_ctas_per_sm(int nmax, int warps, int ring)
 {
-    const void *k = nmax <= 8 ? (const void *)k_lane<8, true, false> : (const void *)k_lane<12, true, false>;
+    if (nmax > 13) return 0;
+    const void *k = nmax <= 8    ? (const void *)k_lane<8, true, false>
+                    : nmax <= 12 ? (const void *)k_lane<12, true, false>
+                                 : (const void *)k_lane<13, true, false>;
     const size_t smem = lane_smem_bytes(nmax, warps, ring);
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         cudaGetLastError();
@@ -587,9 +599,7 @@ __global__ void k_escal_patch(const EscalResult *r, const unsigned long long *co
         if (len) len[e.k] = e.len;
         if (words) {
             uint64_t *w = words + (size_t)e.k * (size_t)ws;
-            w[0] = e.word[0];
-            if (ws > 1) w[1] = e.word[1];
-            for (int j = 2; j < ws; ++j) w[j] = 0ull;
+            for (int j = 0; j < ws; ++j) w[j] = j < 3 ? e.word[j] : 0ull;
         }
     }
 }
@@ -621,6 +631,11 @@ cudaError_t launch_lane(int nmax, int warps, int ring, int refill_k, int tail_k,
         return words ? launch_t<12, true>(warps, ring, refill_k, tail_k, ctas, b, escal_list, escal_capacity,
                                           escal_count, escal_claim, ticket, ls, st)
                      : launch_t<12, false>(warps, ring, refill_k, tail_k, ctas, b, escal_list, escal_capacity,
+                                           escal_count, escal_claim, ticket, ls, st);
+    if (nmax == 13)
+        return words ? launch_t<13, true>(warps, ring, refill_k, tail_k, ctas, b, escal_list, escal_capacity,
+                                          escal_count, escal_claim, ticket, ls, st)
+                     : launch_t<13, false>(warps, ring, refill_k, tail_k, ctas, b, escal_list, escal_capacity,
                                            escal_count, escal_claim, ticket, ls, st);
     return cudaErrorInvalidValue;
 }

@@ -145,6 +145,11 @@ struct Lane {
 
 struct Plan {
     LaneShape lane[2];
+    // a uniform batch of n = 13 (in class 2, whose kernels take 13..16) on the
+    // per-lane kernel k_lane<13> instead of the class's warp-per-automaton
+    // kernel; 0 = off
+    LaneShape lane13;
+    int use_lane13;
     PoolShape pool[3];
     CtaShape cta;
     CtaShape hbm;
