@@ -477,11 +477,14 @@ sbfs_status ensure_plan(sbfs_handle *h)
         ls.ctas = per_sm * sms;
     }
     {
-        // uniform n = 13: 1 KB of bitmap per lane; ring 32 keeps five one-warp CTAs per SM
+        // uniform n = 13: 1 KB of bitmap per lane and a 128-entry ring, three
+        // one-warp CTAs per SM.  2^21 automata: ring 32 3.47 ms, 64 2.48 ms,
+        // 128 2.03 ms, 256 2.60 ms, 512 3.84 ms -- a small ring escalates more
+        // searches to the whole-warp path, a large one costs resident warps
         LaneShape &ls = P.lane13;
         ls.nmax = 13;
         ls.warps = 1;
-        ls.ring = 32;
+        ls.ring = 128;
         ls.refill_k = 16;
         ls.tail_k = 4;
         const int per_sm = lane_max_ctas_per_sm(13, ls.warps, ls.ring);
