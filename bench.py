@@ -576,8 +576,10 @@ def run_sbfs(args):
     line = None
     if rank == 0:
         # roofline of the dominant kernel (the step is one BFS launch plus tiny bookkeeping)
-        kern = [c["kernel"] for c in plan.get("classes", []) if c["max_n"] >= wl["max_n"]][:1]
-        kernel = kern[0] if kern else "k_pool"
+        cls = [c for c in plan.get("classes", []) if c["max_n"] >= wl["max_n"]][:1]
+        kernel = cls[0]["kernel"] if cls else "k_pool"
+        if cls and wl["ns"] is None and wl["n"] == 13 and cls[0].get("uniform_n13"):
+            kernel = cls[0]["uniform_n13"]     # a uniform n = 13 batch runs on the per-lane kernel
         peaks = {}
         try:
             peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))

@@ -477,7 +477,7 @@ sbfs_status ensure_plan(sbfs_handle *h)
         ls.ctas = per_sm * sms;
     }
     {
-        // uniform n = 13: 1 KB of bitmap per lane and a 128-entry ring, three
+        // uniform n = 13: 1 KB of bitmap per lane and a 128-entry ring, four
         // one-warp CTAs per SM.  2^21 automata: ring 32 3.47 ms, 64 2.48 ms,
         // 128 2.03 ms, 256 2.60 ms, 512 3.84 ms -- a small ring escalates more
         // searches to the whole-warp path, a large one costs resident warps
