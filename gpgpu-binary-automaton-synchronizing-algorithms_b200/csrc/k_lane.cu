@@ -134,9 +134,11 @@ __device__ void warp_solve(const Batch &b, int64_t k, uint32_t *region, int lane
     uint32_t *q = region + BW;    // linear queue, 2^NMAX entries
     const int n = automaton_n(b, k);
     const uint8_t *rec = b.maps + (size_t)k * 2u * (size_t)b.lstride;
-    // chunks 0 and 1 in lanes 0-15 / 16-31 of t01, chunks 2 and 3 likewise in t23
+    // chunks 0 and 1 in lanes 0-15 / 16-31 of t01, chunk 2 (and 3) likewise in t23
     const uint32_t t01 = table_entry<NMAX>(rec, b.lstride, n, lane >> 4, lane & 15);
-    const uint32_t t23 = G::kChunks > 2 ? table_entry<NMAX>(rec, b.lstride, n, 2 + (lane >> 4), lane & 15) : 0u;
+    const uint32_t t23 = G::kChunks > 3   ? table_entry<NMAX>(rec, b.lstride, n, 2 + (lane >> 4), lane & 15)
+                         : G::kChunks > 2 ? table_entry<NMAX>(rec, b.lstride, n, 2, lane & 15)
+                                          : 0u;
     for (int w = lane; w < BW; w += 32) bm[w] = 0u;
     __syncwarp();
     const uint32_t full = (1u << n) - 1u;
@@ -214,8 +216,12 @@ __device__ void warp_solve(const Batch &b, int64_t k, uint32_t *region, int lane
             uint64_t *w = b.out_words + (size_t)k * (size_t)b.word_stride;
             w[0] = w0;
             if (b.word_stride > 1) w[1] = w1;
-            if (b.word_stride > 2) w[2] = w2;
-            for (int c = 3; c < b.word_stride; ++c) w[c] = 0ull;
+            if (G::kWordU64 > 2) {
+                if (b.word_stride > 2) w[2] = w2;
+                for (int c = 3; c < b.word_stride; ++c) w[c] = 0ull;
+            } else {
+                for (int c = 2; c < b.word_stride; ++c) w[c] = 0ull;
+            }
         }
         if (STREAM && ls.escal_out) {
             // streamed batches: the host patches escalated automata from here
