@@ -245,9 +245,13 @@ sbfs_status run_level_class(sbfs_handle *h, Lane &L, const Job &j, const Batch &
 }
 
 // A uniform batch of n = 13 runs on the per-lane kernel k_lane<13>.
-bool lane13_batch(const sbfs_handle *h, const uint8_t *ns, int32_t n_uniform)
+// (and of n = 14 on k_lane<14>); the shape, or null
+const LaneShape *uniform_lane(const sbfs_handle *h, const uint8_t *ns, int32_t n_uniform)
 {
-    return h->plan.use_lane13 && !ns && n_uniform == 13;
+    if (ns) return nullptr;
+    if (n_uniform == 13 && h->plan.use_lane13) return &h->plan.lane13;
+    if (n_uniform == 14 && h->plan.use_lane14) return &h->plan.lane14;
+    return nullptr;
 }
 
 // Reserve the lane's work buffers for a job and enqueue its kernels on the lane's
@@ -303,9 +307,10 @@ sbfs_status enqueue_kernels(sbfs_handle *h, Lane &L, const Job &j, int *launches
             CK(cudaStreamWaitEvent(cs, L.ev_fork, 0), "ordering streams");
             joined[c] = true;
         }
-        const bool lane13 = c == 2 && !plain && !ticket_override && lane13_batch(h, j.ns, j.n_uniform);
+        const LaneShape *ul = c == 2 && !plain && !ticket_override ? uniform_lane(h, j.ns, j.n_uniform) : nullptr;
+        const bool lane13 = ul != nullptr;
         if ((c < 2 && !plain && !P.use_pool[c]) || lane13) {
-            const LaneShape &ls = lane13 ? P.lane13 : P.lane[c];
+            const LaneShape &ls = lane13 ? *ul : P.lane[c];
             // one escalation list per lane class (a uniform n = 13 batch has no
             // class 1 and takes its list and counters); entries read as -1 until stored
             const int lc = lane13 ? 1 : c;
@@ -491,6 +496,20 @@ sbfs_status ensure_plan(sbfs_handle *h)
         ls.ctas = per_sm * sms;
         P.use_lane13 = per_sm > 0 && h->cfg.small_kernel != 2 ? 1 : 0;
     }
+    {
+        // uniform n = 14: 2 KB of bitmap per lane and a 256-entry ring, two
+        // one-warp CTAs per SM.  2^21 automata: 4.83 ms (k_hash: 7.80 ms; ring
+        // 128: 5.19 ms; ring 512, one CTA per SM: 9.48 ms)
+        LaneShape &ls = P.lane14;
+        ls.nmax = 14;
+        ls.warps = 1;
+        ls.ring = 256;
+        ls.refill_k = 16;
+        ls.tail_k = 4;
+        const int per_sm = lane_max_ctas_per_sm(14, ls.warps, ls.ring);
+        ls.ctas = per_sm * sms;
+        P.use_lane14 = per_sm > 0 && h->cfg.small_kernel != 2 ? 1 : 0;
+    }
     P.cta.threads = 1024;   // the autotuner's pick with Cerny members in the batch
     P.cta.ctas = sms * 4;
     P.hbm.threads = 512;
@@ -670,7 +689,7 @@ bool stream_eligible(sbfs_handle *h, const uint8_t *ns, int32_t n_uniform, int64
 {
     if (plain || ns || h->cfg.chunk != 0 || count < 2 * kStreamChunk) return false;
     const int c = class_of_n(n_uniform);
-    return (c < 2 && !h->plan.use_pool[c]) || lane13_batch(h, ns, n_uniform);
+    return (c < 2 && !h->plan.use_pool[c]) || uniform_lane(h, ns, n_uniform) != nullptr;
 }
 
 struct StreamOut {
@@ -694,7 +713,7 @@ sbfs_status solve_streamed_job(sbfs_handle *h, const uint8_t *maps, int32_t lstr
     const int c = class_of_n(n);
     // n = 13 (class 2) runs on k_lane<13> with class 1's escalation counters
     const int lc = c < 2 ? c : 1;
-    const LaneShape &ls = c < 2 ? h->plan.lane[c] : h->plan.lane13;
+    const LaneShape &ls = c < 2 ? h->plan.lane[c] : *uniform_lane(h, nullptr, n);
     CK(L.maps.reserve(cnt * rec), "allocating records");
     if (out_len) CK(L.len.reserve(cnt * sizeof(int32_t)), "allocating lengths");
     if (out_words) CK(L.words.reserve((size_t)cnt * ws * sizeof(uint64_t)), "allocating words");
@@ -1471,8 +1490,10 @@ int32_t sbfs_describe_plan(sbfs_handle *h, char *buf, int32_t len)
         if (c == 2 && P.class2_hash && P.use_lane13) {
             std::snprintf(tmp, sizeof tmp,
                           "{\"class\":2,\"max_n\":16,\"kernel\":\"k_hash+k_cta\",\"slots\":%d,"
-                          "\"uniform_n13\":\"k_lane<13>\",\"ring13\":%d,\"ctas13\":%d},",
-                          P.class2_hash == 2 ? 4096 : 2048, P.lane13.ring, P.lane13.ctas);
+                          "\"uniform_n13\":\"k_lane<13>\",\"ring13\":%d,\"ctas13\":%d,"
+                          "\"uniform_n14\":\"%s\",\"ring14\":%d,\"ctas14\":%d},",
+                          P.class2_hash == 2 ? 4096 : 2048, P.lane13.ring, P.lane13.ctas,
+                          P.use_lane14 ? "k_lane<14>" : "k_hash+k_cta", P.lane14.ring, P.lane14.ctas);
         } else if (lane) {
             const LaneShape &l = P.lane[c];
             std::snprintf(tmp, sizeof tmp,

@@ -1,4 +1,4 @@
-// k_lane.cu -- power-set BFS with one automaton per lane (n <= 13).
+// k_lane.cu -- power-set BFS with one automaton per lane (n <= 14).
 //
 // Each lane runs the sequential BFS of GPGPU/CPU/SlimCPU4bits.cs:214-306 on its
 // own automaton: pop subsets, look up both images in its nibble table
@@ -571,15 +571,19 @@ cudaError_t launch_t(int warps, int ring, int refill_k, int tail_k, int ctas, co
 
 size_t lane_smem_bytes(int nmax, int warps, int ring)
 {
-    return nmax <= 8 ? smem_for<8>(warps, ring) : nmax <= 12 ? smem_for<12>(warps, ring) : smem_for<13>(warps, ring);
+    return nmax <= 8    ? smem_for<8>(warps, ring)
+           : nmax <= 12 ? smem_for<12>(warps, ring)
+           : nmax == 13 ? smem_for<13>(warps, ring)
+                        : smem_for<14>(warps, ring);
 }
 
 int lane_max_ctas_per_sm(int nmax, int warps, int ring)
 {
-    if (nmax > 13) return 0;
+    if (nmax > 14) return 0;
     const void *k = nmax <= 8    ? (const void *)k_lane<8, true, false>
                     : nmax <= 12 ? (const void *)k_lane<12, true, false>
-                                 : (const void *)k_lane<13, true, false>;
+                    : nmax == 13 ? (const void *)k_lane<13, true, false>
+                                 : (const void *)k_lane<14, true, false>;
     const size_t smem = lane_smem_bytes(nmax, warps, ring);
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         cudaGetLastError();
@@ -642,6 +646,11 @@ cudaError_t launch_lane(int nmax, int warps, int ring, int refill_k, int tail_k,
         return words ? launch_t<13, true>(warps, ring, refill_k, tail_k, ctas, b, escal_list, escal_capacity,
                                           escal_count, escal_claim, ticket, ls, st)
                      : launch_t<13, false>(warps, ring, refill_k, tail_k, ctas, b, escal_list, escal_capacity,
+                                           escal_count, escal_claim, ticket, ls, st);
+    if (nmax == 14)
+        return words ? launch_t<14, true>(warps, ring, refill_k, tail_k, ctas, b, escal_list, escal_capacity,
+                                          escal_count, escal_claim, ticket, ls, st)
+                     : launch_t<14, false>(warps, ring, refill_k, tail_k, ctas, b, escal_list, escal_capacity,
                                            escal_count, escal_claim, ticket, ls, st);
     return cudaErrorInvalidValue;
 }

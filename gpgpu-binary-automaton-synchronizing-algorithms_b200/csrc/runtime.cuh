@@ -150,6 +150,8 @@ struct Plan {
     // kernel; 0 = off
     LaneShape lane13;
     int use_lane13;
+    LaneShape lane14;    // the same for a uniform batch of n = 14
+    int use_lane14;
     PoolShape pool[3];
     CtaShape cta;
     CtaShape hbm;

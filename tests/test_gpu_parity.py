@@ -81,7 +81,7 @@ def test_tight_records_same_as_64_byte_records(engine):
     np.testing.assert_array_equal(a["len"], b["len"])
 
 
-@pytest.mark.parametrize("n", [3, 5, 8, 9, 12, 13, 16, 17, 20, 21, 24])
+@pytest.mark.parametrize("n", [3, 5, 8, 9, 12, 13, 14, 16, 17, 20, 21, 24])
 def test_cerny_known_answers(engine, n):
     recs = np.stack([P.cerny_record(n)] * 3)
     r = engine.solve(recs, n=n)
