@@ -276,9 +276,9 @@ def test_level_slots_recycle_under_load(oracle_mod):
     assert oracle_mod.replay(recs, r["len"], r["words"], n=21)[0] == 0
 
 
-@pytest.mark.parametrize("n,count", [(12, 300_001), (8, 262_145), (11, 1_000_003), (13, 300_007)])
+@pytest.mark.parametrize("n,count", [(12, 300_001), (8, 262_145), (11, 1_000_003), (13, 300_007), (14, 262_151)])
 def test_streamed_host_path(oracle_mod, n, count):
-    """Uniform n <= 13 batches of at least two 2^17-automaton chunks take the
+    """Uniform n <= 14 batches of at least two 2^17-automaton chunks take the
     streamed host path (one kernel, chunked copies both ways, escalated
     automata patched in at the end); an explicit chunk size takes the
     chunked multi-stream path.  Both must match the oracle."""
@@ -287,13 +287,14 @@ def test_streamed_host_path(oracle_mod, n, count):
         pytest.skip("no CUDA device")
     from sbfs import dotnet_random as D
     recs = D.fill_array_of_problems(count, n, 777 + n, lstride=n)
-    if n == 13:
-        # Cerny C_13 members: 144-letter words, three 64-bit words through the escalation patch
+    if n >= 13:
+        # Cerny C_13 / C_14 members: 144- and 169-letter words, three 64-bit words
+        # through the escalation patch
         for i in (5, 150_001, count - 1):
-            recs[i] = P.repack(P.cerny_record(13)[None, :], 32, 13)[0]
+            recs[i] = P.repack(P.cerny_record(n)[None, :], 32, n)[0]
     ref = oracle_mod.solve(recs, n=n, lstride=n, words=False, threads=8)
-    if n == 13:
-        assert ref["len"][150_001] == 144
+    if n >= 13:
+        assert ref["len"][150_001] == (n - 1) ** 2
     with sbfs.Engine(device=0) as eng, sbfs.Engine(device=0, chunk=1 << 16) as chunked:
         r = eng.solve(recs, n=n, lstride=n)
         _check(oracle_mod, recs, r, n=n, lstride=n, ref=ref)
