@@ -198,6 +198,11 @@ class NvmlClockSampler:
         self.period = period
         self.samples = []
         self.done = threading.Event()
+        # hand the interpreter lock over often enough for the poller to run
+        # while the main thread enqueues steps (the device times are unaffected:
+        # the host runs ahead of the GPU)
+        self.switch = sys.getswitchinterval()
+        sys.setswitchinterval(min(self.switch, period / 5))
         self.thread = threading.Thread(target=self._run, daemon=True)
         self.thread.start()
 
@@ -215,6 +220,7 @@ class NvmlClockSampler:
     def stop(self):
         self.done.set()
         self.thread.join()
+        sys.setswitchinterval(self.switch)
         nv = self.nv
         try:
             nv.nvmlShutdown()
