@@ -531,8 +531,9 @@ sbfs_status ensure_plan(sbfs_handle *h)
 }
 
 sbfs_status check_records(sbfs_handle *h, const uint8_t *maps, int32_t lstride, const uint8_t *ns,
-                          int32_t n_uniform, int64_t count, int32_t *max_n)
+                          int32_t n_uniform, int64_t count, int32_t *max_n, int32_t *same_n = nullptr)
 {
+    if (same_n) *same_n = 0;
     if (count < 0) return fail(h, SBFS_EINVAL, "negative count");
     if (count > 0 && !maps) return fail(h, SBFS_EINVAL, "maps is NULL");
     if (lstride < 1 || lstride > 32) return fail(h, SBFS_EINVAL, "lstride must be in 1..32");
@@ -541,9 +542,14 @@ sbfs_status check_records(sbfs_handle *h, const uint8_t *maps, int32_t lstride, 
             return fail(h, SBFS_EINVAL, "n_uniform must be in 1..min(28, lstride)");
         *max_n = n_uniform;
     } else {
-        int m = 0;
-        for (int64_t i = 0; i < count; ++i) m = std::max<int>(m, ns[i]);
+        int m = 0, lo = 255;
+        for (int64_t i = 0; i < count; ++i) {
+            m = std::max<int>(m, ns[i]);
+            lo = std::min<int>(lo, ns[i]);
+        }
         *max_n = std::min(m, SBFS_MAX_N);
+        // every automaton has the same valid n: the batch is uniform
+        if (same_n && count > 0 && lo == m && m >= 1 && m <= SBFS_MAX_N && m <= lstride) *same_n = m;
     }
     return SBFS_OK;
 }
@@ -963,9 +969,15 @@ sbfs_status solve_host(sbfs_handle *h, const uint8_t *maps, int32_t lstride, con
     std::lock_guard<std::mutex> lock(h->mu);
     h->last_error.clear();
     const auto t0 = std::chrono::steady_clock::now();
-    int32_t max_n = 0;
-    sbfs_status s = check_records(h, maps, lstride, ns, n_uniform, count, &max_n);
+    int32_t max_n = 0, same_n = 0;
+    sbfs_status s = check_records(h, maps, lstride, ns, n_uniform, count, &max_n, &same_n);
     if (s) return s;
+    if (same_n) {
+        // one n for every automaton (the IComputable mirrors always pass sizes):
+        // the uniform-batch kernels and paths apply, and the sizes need not cross
+        ns = nullptr;
+        n_uniform = same_n;
+    }
     if (out_words && word_stride < 1) return fail(h, SBFS_EINVAL, "word_stride must be >= 1");
     if (!out_len && out_words) return fail(h, SBFS_EINVAL, "words need out_len");
     CK(cudaSetDevice(h->device), "selecting device");

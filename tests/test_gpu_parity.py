@@ -548,3 +548,30 @@ def test_streamed_batch_as_a_fresh_process_first_call(oracle_mod, tmp_path):
     ref = oracle_mod.solve(recs, n=n, words=False, threads=8)
     np.testing.assert_array_equal(lens, ref["len"])
     assert oracle_mod.replay(recs, lens, words, n=n)[0] == 0
+
+
+def test_equal_sizes_take_the_uniform_path(engine, oracle_mod):
+    """A per-automaton size array whose entries are all equal (the IComputable
+    mirrors always pass one) runs as a uniform batch: no size bytes cross the
+    link, and the results equal those of the same batch given one n."""
+    count, n = 50_000, 13
+    recs = P.uniform_maps(count, n, 0x5A5A)
+    recs[7] = P.cerny_record(n)
+    ns = np.full(count, n, dtype=np.uint8)
+    r = engine.solve(recs, ns=ns)
+    assert r["stats"]["h2d_bytes"] == count * 64           # records only
+    u = engine.solve(recs, n=n)
+    np.testing.assert_array_equal(r["len"], u["len"])
+    ref = _check(oracle_mod, recs, r, ns=ns)
+    assert ref["len"][7] == (n - 1) ** 2
+    # one size that differs keeps the per-automaton path
+    ns2 = ns.copy()
+    ns2[-1] = 12
+    recs2 = recs.copy()
+    recs2[-1, 12] = 0                                      # state 12 of a is past n = 12: cleared
+    recs2[-1, 32 + 12] = 0
+    recs2[-1, :12] %= 12
+    recs2[-1, 32:44] %= 12
+    r2 = engine.solve(recs2, ns=ns2)
+    assert r2["stats"]["h2d_bytes"] == count * 64 + count
+    _check(oracle_mod, recs2, r2, ns=ns2)
