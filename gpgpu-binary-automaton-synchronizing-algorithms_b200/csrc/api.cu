@@ -666,7 +666,7 @@ std::string graph_key(const void *a, const void *b, const void *c, const void *d
     return buf;
 }
 
-// Streamed host path for a uniform batch of n <= 12 on the per-lane kernel:
+// Streamed host path for a uniform batch of n <= 14 on the per-lane kernel:
 // one kernel launch per job instead of one per chunk (each launch pays the
 // BFS's longest tail), with the copies of both directions overlapping it.
 //  - copy_in: records chunk by chunk, each followed by its chunk_ready flag;
