@@ -61,7 +61,7 @@ struct HostBuf {
     template <class T> T *as() const { return static_cast<T *>(ptr); }
 };
 
-// The streamed host path (uniform n <= 12 on the per-lane kernel): records go
+// The streamed host path (uniform n <= 14 on the per-lane kernels): records go
 // in chunk by chunk on the handle's copy-in stream while one kernel runs, and
 // each chunk's results come back on copy_out as soon as the kernel flags it.
 struct Streamer {

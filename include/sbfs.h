@@ -81,13 +81,14 @@ typedef struct sbfs_config {
     int32_t slots_per_warp;    /* small-n kernel: automata in flight per warp; 0 = auto */
     int32_t warps_per_cta;     /* small-n kernel: warps per CTA; 0 = auto               */
     int32_t queue_smem;        /* small-n kernel: on-chip queue entries per automaton; 0 = auto */
-    int32_t chunk;             /* host path: 0 = auto -- a uniform batch of n <= 12 with at least
+    int32_t chunk;             /* host path: 0 = auto -- a uniform batch of n <= 14 with at least
                                   2^18 automata runs as one kernel while its records stream in
                                   and its results stream out in 2^17-automaton pieces; other
                                   batches in chunks of 2^18 over the streams.  > 0 = chunks of
                                   this many automata over the streams, never streamed      */
-    int32_t small_kernel;      /* n <= 16: 0 = auto (per lane up to n = 12, hash-set warps for 13..16),
-                                  1 = one automaton per lane (n <= 12), 2 = warp-pooled (n <= 16) */
+    int32_t small_kernel;      /* n <= 16: 0 = auto (per lane up to n = 12 and for uniform batches of
+                                  n = 13 or 14, hash-set warps for 13..16), 1 = one automaton per
+                                  lane (n <= 12), 2 = warp-pooled (n <= 16) */
     int32_t lane_ring;         /* per-lane kernel: on-chip frontier entries (power of 2); 0 = auto */
     int32_t lane_refill;       /* per-lane kernel: idle lanes that trigger a refill; 0 = auto */
     int32_t lane_warps;        /* per-lane kernel: warps per CTA; 0 = auto              */
