@@ -63,7 +63,9 @@ cudaError_t launch_level_narrow(int parity, int max_levels, unsigned long long n
                                 uint64_t *tables, LevelCtl *ctl, const Batch &out, cudaStream_t st);
 
 // Level totals at or below this are expanded by one cluster of CTAs looping
-// over levels (k_level_narrow).
+// over levels (k_level_narrow).  Raising it to 32768 or 65536 made C_28 slower
+// (12.78 and 13.86 ms against 12.51): eight SMs take longer over those levels
+// than the whole grid's launch costs.
 constexpr unsigned long long kNarrowLevel = 16384;
 
 // First-fit allocator over one device buffer (host-side bookkeeping only).
