@@ -43,6 +43,11 @@
 // warp writes their results and loads new automata for all of them in one
 // pass, so the per-automaton set-up (record load, table build, bitmap clear)
 // runs with many lanes active instead of one.
+//
+// Instances: NMAX = 8 and 12 for size classes 0 and 1; 13 and 14 for uniform
+// batches of that n (a fourth nibble chunk, 1 or 2 KB of bitmap per lane, and
+// words of up to (NMAX - 1)^2 = 144 or 169 letters -- three 64-bit words -- in
+// the whole-warp search).
 #include "common.cuh"
 
 namespace sbfs {
