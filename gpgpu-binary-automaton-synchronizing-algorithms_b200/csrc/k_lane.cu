@@ -55,6 +55,10 @@ namespace {
 
 constexpr int kActive = 0, kDone = 1, kEscalate = 2, kIdle = 3, kHeld = 4;
 constexpr int kStep = 4;   // subsets a lane expands per step (their 2 * kStep images are tested together)
+// At n = 13 and 14 fewer warps fit on an SM (four, two), and six subsets per
+// step hide more of each warp's latency: 2^21 automata at n = 14 4.83 -> 4.64 ms,
+// the n = 13 streamed kernel 2.19 -> 2.09 ms (eight: no better than six)
+constexpr int kStepWide = 6;
 
 __host__ __device__ constexpr int low_bit4(int v)
 {
@@ -472,7 +476,7 @@ __global__ void __launch_bounds__(256) k_lane(Batch b, int ring, int refill_k, i
             // a lane with fewer than kStep subsets left in the level expands its
             // first one again in the spare places: those copies' images are
             // already visited by the time they are tested
-            constexpr int P = kStep;
+            constexpr int P = NMAX >= 13 ? kStepWide : kStep;
             const uint32_t take = min(lvl_end - head, (uint32_t)P);
             uint32_t e[P];
 #pragma unroll
